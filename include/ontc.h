@@ -1,0 +1,236 @@
+/*
+ * ontc.h -- C ABI of the B200 neural-texture-compression library (libontc.so).
+ *
+ * This is the drop-in boundary for openntc's libopenntc: every entry point below
+ * replaces one member of upstream's openntc::Context (libopenntc/libopenntc.h:168-197)
+ * or one free function of its CUDA-free runtime (libopenntc/openntc_runtime.h:55-150).
+ * The structs are byte-compatible with upstream's (same field order, same sizes), so a
+ * CompressedData produced by either side can be handed to the other.  The header-only
+ * C++ wrapper in include/libopenntc/ puts upstream's class and function names on top.
+ *
+ * Conventions
+ *  - Status returns are upstream's openntc::Result values (openntc_runtime.h:18-30).
+ *  - One context = one GPU = one CUDA stream.  Not thread-safe; callers serialise, as
+ *    upstream's GUI does (openntc-gui/thread.h:15-28).
+ *  - All compute runs on hand-written sm_100a kernels inside libontc.so.  There is no
+ *    CPU fallback: with no usable GPU, ontc_init returns ONTC_CUDA_FAILURE.
+ */
+#ifndef ONTC_H_
+#define ONTC_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ONTC_MAX_MIPS 12     /* openntc_runtime.h:51 kMaxMips */
+#define ONTC_MAX_CHANNELS 16 /* openntc_runtime.h:52 kMaxChannels */
+#define ONTC_MAX_LEVELS 6    /* openntc_runtime.h:53 kMaxLevels */
+#define ONTC_MAX_SOURCES 16  /* libopenntc.h:138 kMaxSources */
+#define ONTC_MIN_DIMENSION 1024 /* libopenntc.h:171 kMinDimension (see ontc_set_min_dimension) */
+#define ONTC_MAX_DIMENSION 8192 /* libopenntc.h:172 kMaxDimension */
+
+/* openntc::Result, openntc_runtime.h:18-30 */
+enum {
+  ONTC_SUCCESS = 0,
+  ONTC_INVALID_DIMENSION = 1,
+  ONTC_ALLOCATION_FAILURE = 2,
+  ONTC_INVALID_MANIFEST = 3,
+  ONTC_FILE_NOT_FOUND = 4,
+  ONTC_INVALID_FILE = 5,
+  ONTC_FILE_WRITE_FAILURE = 6,
+  ONTC_INVALID_STATE = 7,
+  ONTC_CUDA_FAILURE = 8
+};
+
+/* openntc::Profile, openntc_runtime.h:8-16 */
+enum { ONTC_BPP_0_2 = 0, ONTC_BPP_0_5 = 1, ONTC_BPP_1_0 = 2, ONTC_BPP_2_25 = 3 };
+
+/* openntc::Quality, libopenntc.h:147-155 */
+enum { ONTC_QUALITY_LOW = 0, ONTC_QUALITY_MEDIUM = 1, ONTC_QUALITY_HIGH = 2, ONTC_QUALITY_ULTRA = 3 };
+
+/* openntc::TrainPhase, libopenntc.h:99-106 */
+enum { ONTC_MANIFEST_LOADED = 0, ONTC_TRAIN_IN_PROGRESS = 1, ONTC_TRAIN_COMPLETE = 2, ONTC_TRAIN_ERROR = -1 };
+
+/* MLP arithmetic of the training step (no upstream counterpart: upstream always runs
+ * cuBLAS TF32, libopenntc.cpp:374).
+ *   BF16 (default): tcgen05/TMEM bf16 operands, fp32 accumulate, fp32 master weights and
+ *                   fp32 Adam moments.
+ *   FP32:           SIMT fp32 tile kernel (the plain comparator). */
+enum { ONTC_PRECISION_BF16 = 0, ONTC_PRECISION_FP32 = 1 };
+
+/* Decoder arithmetic for ontc_decode (upstream: HLSL only, ntc_decode.hlsli:605-623). */
+enum {
+  ONTC_DECODE_INT8 = 0, /* SampleMaterial semantics, integer-exact with the DP4A path */
+  ONTC_DECODE_FP32 = 1, /* float model, fp32 weights */
+  ONTC_DECODE_BF16 = 2, /* float model, bf16 weights and activations */
+  ONTC_DECODE_FP8 = 3   /* float model, e4m3 weights with per-layer scales */
+};
+
+/* openntc::CalibrationData, openntc_runtime.h:61-67 */
+typedef struct ontc_calibration {
+  float max_abs_a1;
+  float max_abs_a2;
+  float s_a1;
+  float s_a2;
+} ontc_calibration;
+
+/* openntc::NTCConstants, openntc_runtime.h:69-89 (240 bytes; HLSL cbuffer NTC) */
+typedef struct ontc_constants {
+  int32_t g0_grid_dim[8];
+  int32_t g1_grid_dim[8];
+  uint32_t g0_offset[8];
+  uint32_t g1_offset[8];
+  int32_t g0_bits_per_channel;
+  int32_t g1_bits_per_channel;
+  int32_t g0_channels;
+  int32_t g1_channels;
+  int32_t dim;
+  int32_t mip_count;
+  float rcp_s_a1;
+  float rcp_s_a2;
+  int32_t channel_count;
+  int32_t pad0[3];
+  uint32_t channel_semantics[16];
+} ontc_constants;
+
+/* openntc::CompressedData, openntc_runtime.h:91-121.  Pointers are borrowed (owned by a
+ * context or by an ontc_file). */
+typedef struct ontc_compressed_data {
+  uint32_t* g0[ONTC_MAX_LEVELS];
+  uint32_t* g1[ONTC_MAX_LEVELS];
+  void* decoder;
+  size_t g0_size[ONTC_MAX_LEVELS];
+  size_t g1_size[ONTC_MAX_LEVELS];
+  size_t g0_offset[ONTC_MAX_LEVELS];
+  size_t g1_offset[ONTC_MAX_LEVELS];
+  size_t g0_total_size;
+  size_t g1_total_size;
+  size_t decoder_size;
+  int32_t g0_grid_dim[ONTC_MAX_LEVELS];
+  int32_t g1_grid_dim[ONTC_MAX_LEVELS];
+  int32_t g0_bits_per_channel;
+  int32_t g1_bits_per_channel;
+  int32_t g0_channels;
+  int32_t g1_channels;
+  int32_t dim;
+  int32_t mip_count;
+  int32_t level_count;
+  int32_t channel_count;
+  int32_t channel_semantics[ONTC_MAX_CHANNELS];
+  int32_t profile;
+  ontc_calibration caldata;
+} ontc_compressed_data;
+
+/* openntc::TrainProgress, libopenntc.h:108-114 */
+typedef struct ontc_train_progress {
+  int32_t phase;
+  int32_t result;
+  int32_t batches_complete;
+  int32_t total_batches;
+} ontc_train_progress;
+
+/* openntc::EvalResults, libopenntc.h:93-97 */
+typedef struct ontc_eval_results {
+  double mse;
+  double psnr;
+} ontc_eval_results;
+
+/* openntc::TextureData, libopenntc.h:325-332 */
+typedef struct ontc_texture_data {
+  int32_t tex_count;
+  int32_t mip_count;
+  int32_t channels[ONTC_MAX_SOURCES];
+  int32_t semantics[ONTC_MAX_SOURCES];
+  uint8_t* mips[ONTC_MAX_SOURCES][ONTC_MAX_MIPS];
+} ontc_texture_data;
+
+/* Options with no upstream counterpart; zero-initialise and set what you need, then pass
+ * to ontc_set_train_options after ontc_begin_training and before the first ontc_train.
+ * An all-zero struct keeps upstream's schedule and the default (BF16) arithmetic. */
+typedef struct ontc_train_options {
+  int32_t steps_override; /* >0: total steps instead of the quality preset; lock moves to 95 % of it */
+  int32_t has_lock_step;  /* !=0: use lock_step as the latent lock/snap step */
+  int32_t lock_step;
+  int32_t precision;      /* ONTC_PRECISION_* */
+  int32_t reserved[4];
+} ontc_train_options;
+
+typedef struct ontc_context ontc_context;
+typedef struct ontc_file ontc_file;
+typedef struct ontc_decoder ontc_decoder;
+
+/* ---- Context lifecycle (libopenntc.h:177-197) ---------------------------------------- */
+
+/* Context::Context (libopenntc.cpp:271): host RNG std::mt19937(123). */
+ontc_context* ontc_create(void);
+/* Context::~Context + Destroy (libopenntc.cpp:1443) */
+void ontc_destroy(ontc_context* ctx);
+/* Context::Init (libopenntc.cpp:280).  `stream` is a cudaStream_t (NULL: a private stream). */
+int ontc_init(ontc_context* ctx, int32_t profile, void* stream);
+/* No upstream counterpart: lowers the manifest's minimum texture size (upstream fixes it
+ * at 1024, libopenntc.h:171) to any power of two >= 16.  Call before ontc_load_manifest. */
+int ontc_set_min_dimension(ontc_context* ctx, int32_t dim);
+/* Context::LoadManifest (libopenntc.cpp:1125) */
+int ontc_load_manifest(ontc_context* ctx, const char* path);
+/* Context::UnloadManifest (libopenntc.cpp:1369) */
+void ontc_unload_manifest(ontc_context* ctx);
+/* Context::BeginTraining (libopenntc.cpp:471) */
+void ontc_begin_training(ontc_context* ctx, int32_t quality, int32_t grids_per_batch);
+/* No upstream counterpart (upstream sets these only through Quality). */
+int ontc_set_train_options(ontc_context* ctx, const ontc_train_options* opts);
+/* Context::Train (libopenntc.cpp:536) */
+void ontc_train(ontc_context* ctx, int32_t num_batches, ontc_train_progress* out);
+/* Context::TrainUntilComplete (libopenntc.cpp:529) */
+void ontc_train_until_complete(ontc_context* ctx, ontc_train_progress* out);
+/* Context::Eval (libopenntc.cpp:972).  FP64 reduction. */
+void ontc_eval(ontc_context* ctx, ontc_eval_results* out);
+/* Context::Calibrate (libopenntc.cpp:898) */
+void ontc_calibrate(ontc_context* ctx, float headroom, ontc_calibration* out);
+/* Context::GetCompressedData (libopenntc.cpp:1055) */
+void ontc_get_compressed_data(ontc_context* ctx, ontc_compressed_data* out);
+/* Context::GetTextureData (libopenntc.cpp:1425) */
+void ontc_get_texture_data(ontc_context* ctx, ontc_texture_data* out);
+/* Context::GetMipDim (libopenntc.cpp:1495) */
+int32_t ontc_get_mip_dim(ontc_context* ctx, int32_t mip);
+/* Context::FeatureLevelForLod (libopenntc.cpp:881) */
+int32_t ontc_feature_level_for_lod(ontc_context* ctx, int32_t lod);
+/* Context::GetLastError (libopenntc.cpp:893) */
+int ontc_get_last_error(ontc_context* ctx);
+/* GetStepsForQuality (libopenntc.cpp:428) */
+int32_t ontc_steps_for_quality(int32_t quality);
+/* Mean loss (sum of squared residuals / (C*B)) of the last `n` completed steps, FP64;
+ * upstream computes this per step and discards it (libopenntc.cpp:662-663). */
+int ontc_get_step_losses(ontc_context* ctx, double* out, int32_t n);
+
+/* ---- Runtime (openntc_runtime.h:55-150) ---------------------------------------------- */
+
+/* FillNTCConstants (openntc_runtime.cpp:156) */
+void ontc_fill_constants(const ontc_compressed_data* data, ontc_constants* out);
+/* Dump (openntc_runtime.cpp:179): writes the ONTC container. */
+int ontc_dump(const char* path, const ontc_compressed_data* data);
+/* Load (openntc_runtime.cpp:307) + FileData (openntc_runtime.h:131-150).  On success *file
+ * owns the bytes `out` points into; release with ontc_file_free even on failure. */
+int ontc_load(const char* path, ontc_file** file, ontc_compressed_data* out);
+void ontc_file_free(ontc_file* file);
+/* ProfileToString / ProfileFromString / SemanticToString / SemanticFromName /
+ * GetChannelCountForSemantic (openntc_runtime.cpp:20-154) */
+const char* ontc_profile_to_string(int32_t profile);
+int ontc_profile_from_string(const char* s, int32_t* out_profile);
+const char* ontc_semantic_to_string(int32_t semantic);
+int32_t ontc_semantic_from_name(const char* name);
+int32_t ontc_channel_count_for_semantic(int32_t semantic);
+
+/* ---- Library facts --------------------------------------------------------------------- */
+
+/* Number of kernel launches this context issued so far (all of them are libontc's own). */
+int64_t ontc_kernel_launch_count(ontc_context* ctx);
+/* Version string of the build ("ontc <git-describe> sm_100a"). */
+const char* ontc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ONTC_H_ */

@@ -1,0 +1,133 @@
+"""ctypes mirror of include/ontc.h (the C ABI of libontc.so).
+
+Struct layouts here must stay byte-identical to the C header; tests check sizes and
+offsets against the C compiler's view.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+MAX_MIPS = 12
+MAX_CHANNELS = 16
+MAX_LEVELS = 6
+MAX_SOURCES = 16
+
+SUCCESS, INVALID_DIMENSION, ALLOCATION_FAILURE, INVALID_MANIFEST, FILE_NOT_FOUND, \
+    INVALID_FILE, FILE_WRITE_FAILURE, INVALID_STATE, CUDA_FAILURE = range(9)
+RESULT_NAMES = ["Success", "InvalidDimension", "AllocationFailure", "InvalidManifest", "FileNotFound",
+                "InvalidFile", "FileWriteFailure", "InvalidState", "CudaFailure"]
+
+BPP_0_2, BPP_0_5, BPP_1_0, BPP_2_25 = range(4)
+QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH, QUALITY_ULTRA = range(4)
+MANIFEST_LOADED, TRAIN_IN_PROGRESS, TRAIN_COMPLETE, TRAIN_ERROR = 0, 1, 2, -1
+PRECISION_BF16, PRECISION_FP32 = 0, 1
+DECODE_INT8, DECODE_FP32, DECODE_BF16, DECODE_FP8 = range(4)
+
+
+class Calibration(C.Structure):
+    _fields_ = [("max_abs_a1", C.c_float), ("max_abs_a2", C.c_float), ("s_a1", C.c_float), ("s_a2", C.c_float)]
+
+
+class Constants(C.Structure):
+    _fields_ = [
+        ("g0_grid_dim", C.c_int32 * 8), ("g1_grid_dim", C.c_int32 * 8),
+        ("g0_offset", C.c_uint32 * 8), ("g1_offset", C.c_uint32 * 8),
+        ("g0_bits_per_channel", C.c_int32), ("g1_bits_per_channel", C.c_int32),
+        ("g0_channels", C.c_int32), ("g1_channels", C.c_int32),
+        ("dim", C.c_int32), ("mip_count", C.c_int32),
+        ("rcp_s_a1", C.c_float), ("rcp_s_a2", C.c_float),
+        ("channel_count", C.c_int32), ("pad0", C.c_int32 * 3),
+        ("channel_semantics", C.c_uint32 * 16),
+    ]
+
+
+class CompressedData(C.Structure):
+    _fields_ = [
+        ("g0", C.POINTER(C.c_uint32) * MAX_LEVELS), ("g1", C.POINTER(C.c_uint32) * MAX_LEVELS),
+        ("decoder", C.c_void_p),
+        ("g0_size", C.c_size_t * MAX_LEVELS), ("g1_size", C.c_size_t * MAX_LEVELS),
+        ("g0_offset", C.c_size_t * MAX_LEVELS), ("g1_offset", C.c_size_t * MAX_LEVELS),
+        ("g0_total_size", C.c_size_t), ("g1_total_size", C.c_size_t), ("decoder_size", C.c_size_t),
+        ("g0_grid_dim", C.c_int32 * MAX_LEVELS), ("g1_grid_dim", C.c_int32 * MAX_LEVELS),
+        ("g0_bits_per_channel", C.c_int32), ("g1_bits_per_channel", C.c_int32),
+        ("g0_channels", C.c_int32), ("g1_channels", C.c_int32),
+        ("dim", C.c_int32), ("mip_count", C.c_int32), ("level_count", C.c_int32), ("channel_count", C.c_int32),
+        ("channel_semantics", C.c_int32 * MAX_CHANNELS),
+        ("profile", C.c_int32),
+        ("caldata", Calibration),
+    ]
+
+
+class TrainProgress(C.Structure):
+    _fields_ = [("phase", C.c_int32), ("result", C.c_int32), ("batches_complete", C.c_int32), ("total_batches", C.c_int32)]
+
+
+class EvalResults(C.Structure):
+    _fields_ = [("mse", C.c_double), ("psnr", C.c_double)]
+
+
+class TextureData(C.Structure):
+    _fields_ = [
+        ("tex_count", C.c_int32), ("mip_count", C.c_int32),
+        ("channels", C.c_int32 * MAX_SOURCES), ("semantics", C.c_int32 * MAX_SOURCES),
+        ("mips", (C.POINTER(C.c_uint8) * MAX_MIPS) * MAX_SOURCES),
+    ]
+
+
+class TrainOptions(C.Structure):
+    _fields_ = [("steps_override", C.c_int32), ("has_lock_step", C.c_int32), ("lock_step", C.c_int32),
+                ("precision", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+# name -> (restype, argtypes); every symbol include/ontc.h declares.
+P = C.c_void_p
+SIGNATURES = {
+    "ontc_create": (P, []),
+    "ontc_destroy": (None, [P]),
+    "ontc_init": (C.c_int, [P, C.c_int32, P]),
+    "ontc_set_min_dimension": (C.c_int, [P, C.c_int32]),
+    "ontc_load_manifest": (C.c_int, [P, C.c_char_p]),
+    "ontc_unload_manifest": (None, [P]),
+    "ontc_begin_training": (None, [P, C.c_int32, C.c_int32]),
+    "ontc_set_train_options": (C.c_int, [P, C.POINTER(TrainOptions)]),
+    "ontc_train": (None, [P, C.c_int32, C.POINTER(TrainProgress)]),
+    "ontc_train_until_complete": (None, [P, C.POINTER(TrainProgress)]),
+    "ontc_eval": (None, [P, C.POINTER(EvalResults)]),
+    "ontc_calibrate": (None, [P, C.c_float, C.POINTER(Calibration)]),
+    "ontc_get_compressed_data": (None, [P, C.POINTER(CompressedData)]),
+    "ontc_get_texture_data": (None, [P, C.POINTER(TextureData)]),
+    "ontc_get_mip_dim": (C.c_int32, [P, C.c_int32]),
+    "ontc_feature_level_for_lod": (C.c_int32, [P, C.c_int32]),
+    "ontc_get_last_error": (C.c_int, [P]),
+    "ontc_steps_for_quality": (C.c_int32, [C.c_int32]),
+    "ontc_get_step_losses": (C.c_int, [P, C.POINTER(C.c_double), C.c_int32]),
+    "ontc_fill_constants": (None, [C.POINTER(CompressedData), C.POINTER(Constants)]),
+    "ontc_dump": (C.c_int, [C.c_char_p, C.POINTER(CompressedData)]),
+    "ontc_load": (C.c_int, [C.c_char_p, C.POINTER(P), C.POINTER(CompressedData)]),
+    "ontc_file_free": (None, [P]),
+    "ontc_profile_to_string": (C.c_char_p, [C.c_int32]),
+    "ontc_profile_from_string": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "ontc_semantic_to_string": (C.c_char_p, [C.c_int32]),
+    "ontc_semantic_from_name": (C.c_int32, [C.c_char_p]),
+    "ontc_channel_count_for_semantic": (C.c_int32, [C.c_int32]),
+    "ontc_kernel_launch_count": (C.c_int64, [P]),
+    "ontc_version": (C.c_char_p, []),
+}
+
+
+def declared_symbols(header: Path) -> list[str]:
+    """Function names declared in a C header (one declaration per line starting a type)."""
+    import re
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(ontc_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def bind(lib: C.CDLL) -> C.CDLL:
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib

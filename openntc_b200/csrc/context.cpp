@@ -1,0 +1,945 @@
+// The training context behind the C ABI: upstream's openntc::Context
+// (libopenntc/libopenntc.cpp) re-built around libontc's kernels.
+//
+// What is kept from upstream, because results depend on it:
+//   * profile constants, feature/mip/level geometry (libopenntc.cpp:289-338, 1209-1227);
+//   * one std::mt19937(123) per context, consumed in upstream's order: latents U(-0.1, 0.1)
+//     level by level (g0 then g1), Kaiming-uniform W0, W1, Wout (:483-501), then per step
+//     bernoulli(0.05), U(0,1), uniform lod, and the tile origins (:564-583);
+//   * the schedule: cosine-annealed learning rates, global-step bias correction for the
+//     decoder and per-level step counters for the latents (:711-720), latent lock and
+//     quantisation at 95 % of the steps (:475, :601-619);
+//   * completion: quantise+pack every level, calibrate, int8 per-row weight quantisation
+//     into the decoder blob (:799-876).
+// What changes: two launches per step (a fused tile kernel and a fused optimiser pass)
+// on one stream, the step's draws uploaded in batches ahead of time, no host sync per step,
+// quantisation noise generated at the touched latents only, FP64 loss and PSNR sums.
+#include <algorithm>
+#include <bit>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iterator>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ontc.h"
+#include "image.h"
+#include "json.h"
+#include "kernels.h"
+
+using namespace ontc;
+
+namespace {
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count)
+  {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+    }
+    return e;
+  }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+struct Source {
+  std::string path, name;
+  bool srgb = false, vflip = false;
+  int32_t sem = 0;
+  int32_t nch = 0;
+  int32_t cmap[4] = {-1, -1, -1, -1};
+};
+
+int round_up(int n, int k) { return ((n + k - 1) / k) * k; }
+
+float cosine_annealing(float lr_min, float lr_max, int t_max, int t_cur)
+{
+  // libopenntc.cpp:419-423
+  return lr_min + 0.5f * (lr_max - lr_min) * (1.0f + cosf(t_cur * acosf(-1.0f) / t_max));
+}
+
+// libopenntc.cpp:445-469: per-row symmetric int8 (round half away from zero), scale*prescale.
+void quantize_weights(const float* Wf, int rows, int cols, float prescale, uint32_t* Wq, float* Ws)
+{
+  for (int i = 0; i < rows; i++) {
+    float max_abs = 0.0f;
+    for (int j = 0; j < cols; j++) max_abs = std::max(std::abs(Wf[i * cols + j]), max_abs);
+    const float scale = (max_abs == 0.0f) ? 1.0f : max_abs / 127.0f;
+    Ws[i] = scale * prescale;
+    for (int j = 0; j < cols; j += 4) {
+      uint32_t pack = 0;
+      for (int c = 0; c < 4; c++) {
+        const float val = Wf[i * cols + j + c] / scale;
+        const int q = std::clamp((int)std::lroundf(val), -128, 127);
+        pack |= ((uint32_t)(q & 0xFF) << (c * 8));
+      }
+      Wq[i * (cols / 4) + (j / 4)] = pack;
+    }
+  }
+}
+
+// libopenntc.cpp:1103-1121
+bool valid_semantic_channels(int32_t sem, const std::string& ch)
+{
+  static const char* rgba = "RGBA";
+  if (ch.empty() || ch.size() > 4) return false;
+  int p = 0;
+  for (char c : ch) {
+    while (p < 4 && rgba[p] != c) p++;
+    if (p >= 4) return false;
+    p++;
+  }
+  if (sem != 0 && ontc_channel_count_for_semantic(sem) != (int)ch.size()) return false;
+  return true;
+}
+
+uint32_t step_seed(uint32_t step)
+{
+  // splitmix-style scramble of the step index: distinct noise streams per step
+  uint32_t z = step * 0x9E3779B9u + 0x4F4E5443u;
+  z = (z ^ (z >> 16)) * 0x85EBCA6Bu;
+  z = (z ^ (z >> 13)) * 0xC2B2AE35u;
+  return z ^ (z >> 16);
+}
+
+}  // namespace
+
+struct ontc_context {
+  bool initialized = false;
+  bool manifest_loaded = false;
+  int32_t train_phase = ONTC_MANIFEST_LOADED;
+  int last_error = ONTC_SUCCESS;
+  int min_dimension = ONTC_MIN_DIMENSION;
+
+  // profile
+  int32_t profile = 0, b0 = 0, b1 = 0, C0 = 0, C1 = 0, scale = 0;
+  float d0 = 0.f, d1 = 0.f;
+  int32_t F = 0, Fp = 0, C = 0, nW = 0;
+
+  // geometry
+  int32_t mips = 0, levels = 0;
+  int32_t mip_dim[ONTC_MAX_MIPS] = {};
+  int32_t g0_dim[ONTC_MAX_LEVELS] = {}, g1_dim[ONTC_MAX_LEVELS] = {};
+
+  // training run
+  int32_t batch_count = 0, batch_i = 0, lock_i = 0, grids = 1;
+  int32_t grid_batch_i[ONTC_MAX_LEVELS] = {};
+  int32_t precision = ONTC_PRECISION_BF16;
+  uint32_t last_seed = 0;
+  bool last_noise = false;
+  std::mt19937 gen{123};
+
+  // device
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sms = 148;
+  int max_grid = 148;
+  DBuf<float> lat[2][4][ONTC_MAX_LEVELS];  // [g0/g1][p,m,v,g][level]
+  DBuf<float> W, Wm, Wv, dWpart, calib;
+  DBuf<double> loss_part, losses, eval_sums;
+  DBuf<StepRec> steps, aux_steps;
+  DBuf<uint8_t> package[ONTC_MAX_MIPS];
+  DBuf<uint32_t> packbuf;
+  DBuf<int> tc_error;
+  StepRec* h_steps = nullptr;  // pinned staging
+  size_t h_steps_cap = 0;
+
+  // host outputs (libopenntc.h:201-210)
+  std::vector<uint32_t> g0_host_packed, g1_host_packed;
+  uint32_t* g0_host[ONTC_MAX_LEVELS] = {};
+  uint32_t* g1_host[ONTC_MAX_LEVELS] = {};
+  std::vector<uint8_t> decoder_host;
+  ontc_calibration caldata = {};
+  Source sources[ONTC_MAX_SOURCES];
+  int32_t source_count = 0;
+  std::vector<uint8_t> mips_host[ONTC_MAX_SOURCES][ONTC_MAX_MIPS];
+
+  int64_t launches = 0;
+
+  Model model() const
+  {
+    Model M = {};
+    M.C0 = C0;
+    M.C1 = C1;
+    M.F = F;
+    M.Fp = Fp;
+    M.C = C;
+    M.mips = mips;
+    M.levels = levels;
+    for (int i = 0; i < mips; i++) {
+      M.mip_dim[i] = mip_dim[i];
+      M.package[i] = package[i].p;
+    }
+    for (int g = 0; g < 2; g++) {
+      Pyramid& P = g == 0 ? M.g0 : M.g1;
+      for (int l = 0; l < levels; l++) {
+        P.p[l] = lat[g][0][l].p;
+        P.m[l] = lat[g][1][l].p;
+        P.v[l] = lat[g][2][l].p;
+        P.g[l] = lat[g][3][l].p;
+        P.dim[l] = g == 0 ? g0_dim[l] : g1_dim[l];
+      }
+      P.channels = g == 0 ? C0 : C1;
+      P.bits = g == 0 ? b0 : b1;
+      P.delta = g == 0 ? d0 : d1;
+    }
+    M.W = W.p;
+    M.Wm = Wm.p;
+    M.Wv = Wv.p;
+    M.nW = nW;
+    return M;
+  }
+
+  size_t level_elems(int g, int l) const
+  {
+    const size_t d = (size_t)(g == 0 ? g0_dim[l] : g1_dim[l]);
+    return d * d * (size_t)(g == 0 ? C0 : C1);
+  }
+
+  int32_t feature_level_for_lod(int32_t lod) const
+  {
+    // libopenntc.cpp:881-891
+    const int first = (int)log2f((float)scale) + 2;
+    if (lod < first) return 0;
+    return std::min(1 + (lod - first) / 2, levels - 1);
+  }
+};
+
+namespace {
+
+bool ensure_host_steps(ontc_context* c, size_t n)
+{
+  if (c->h_steps_cap >= n) return true;
+  if (c->h_steps) cudaFreeHost(c->h_steps);
+  c->h_steps = nullptr;
+  c->h_steps_cap = 0;
+  if (cudaMallocHost(&c->h_steps, n * sizeof(StepRec)) != cudaSuccess) return false;
+  c->h_steps_cap = n;
+  return true;
+}
+
+// Full-mip "step" used by Eval and Calibrate: every texel of the mip once.
+StepRec full_mip_rec(const ontc_context* c, int mip)
+{
+  StepRec s = {};
+  s.lod = mip;
+  s.level = c->feature_level_for_lod(mip);
+  s.mip_dim = c->mip_dim[mip];
+  s.tile_dim = c->mip_dim[mip];
+  s.n_grids = 1;
+  s.texels = c->mip_dim[mip] * c->mip_dim[mip];
+  s.noise = c->last_noise ? 1 : 0;
+  s.seed = c->last_seed;
+  s.norm_lod = mip / static_cast<float>(c->mips - 1);
+  s.step = 0;
+  return s;
+}
+
+void unload(ontc_context* c)
+{
+  if (!c->manifest_loaded) return;
+  for (int g = 0; g < 2; g++)
+    for (int k = 0; k < 4; k++)
+      for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->lat[g][k][l].release();
+  for (int i = 0; i < ONTC_MAX_MIPS; i++) c->package[i].release();
+  c->packbuf.release();
+  c->losses.release();
+  c->g0_host_packed.clear();
+  c->g1_host_packed.clear();
+  for (int i = 0; i < ONTC_MAX_LEVELS; i++) c->g0_host[i] = c->g1_host[i] = nullptr;
+  for (int s = 0; s < ONTC_MAX_SOURCES; s++)
+    for (int m = 0; m < ONTC_MAX_MIPS; m++) c->mips_host[s][m].clear();
+  c->manifest_loaded = false;
+}
+
+ontc_train_progress make_progress(int32_t phase, int32_t result, const ontc_context* c)
+{
+  ontc_train_progress p = {};
+  p.phase = phase;
+  p.result = result;
+  p.batches_complete = c->batch_i;
+  p.total_batches = c->batch_count;
+  return p;
+}
+
+// Runs the forward over every texel of every mip (Eval / Calibrate, libopenntc.cpp:898-1053).
+cudaError_t full_forward(ontc_context* c, int mode, std::vector<double>* sums)
+{
+  const Model M = c->model();
+  for (int mip = 0; mip < c->mips; mip++) c->h_steps[mip] = full_mip_rec(c, mip);
+  cudaError_t e = cudaMemcpyAsync(c->aux_steps.p, c->h_steps, c->mips * sizeof(StepRec), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return e;
+  if (mode == kCalib) {
+    e = cudaMemsetAsync(c->calib.p, 0, 2 * sizeof(float), c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  for (int mip = 0; mip < c->mips; mip++) {
+    const int units = (c->mip_dim[mip] * c->mip_dim[mip] + kTile - 1) / kTile;
+    const int grid = std::min(units, c->sms);
+    TileOut out = {c->dWpart.p, c->loss_part.p, c->calib.p};
+    e = launch_simt_units(mode, M, c->aux_steps.p, mip, grid, out, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return e;
+    if (mode == kEval) {
+      e = launch_sum_doubles(c->loss_part.p, grid, c->eval_sums.p + mip, c->stream);
+      c->launches++;
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (mode == kEval) {
+    sums->assign(c->mips, 0.0);
+    e = cudaMemcpyAsync(sums->data(), c->eval_sums.p, c->mips * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaStreamSynchronize(c->stream);
+}
+
+ontc_calibration calibrate(ontc_context* c, float headroom, cudaError_t* err)
+{
+  ontc_calibration cal = {};
+  *err = full_forward(c, kCalib, nullptr);
+  if (*err != cudaSuccess) return cal;
+  float hmax[2] = {0.f, 0.f};
+  *err = cudaMemcpy(hmax, c->calib.p, sizeof(hmax), cudaMemcpyDeviceToHost);
+  if (*err != cudaSuccess) return cal;
+  cal.max_abs_a1 = hmax[0];
+  cal.max_abs_a2 = hmax[1];
+  cal.s_a1 = headroom * hmax[0] / 127.0f;
+  cal.s_a2 = headroom * hmax[1] / 127.0f;
+  return cal;
+}
+
+// Training completion (libopenntc.cpp:799-876).
+cudaError_t complete_training(ontc_context* c)
+{
+  cudaError_t e;
+  for (int l = 0; l < c->levels; l++) {
+    for (int g = 0; g < 2; g++) {
+      const size_t n = c->level_elems(g, l);
+      const int bits = g == 0 ? c->b0 : c->b1;
+      e = launch_quantize_pack(c->lat[g][0][l].p, (long long)n, bits, c->packbuf.p, c->stream);
+      c->launches++;
+      if (e != cudaSuccess) return e;
+      uint32_t* dst = g == 0 ? c->g0_host[l] : c->g1_host[l];
+      e = cudaMemcpyAsync(dst, c->packbuf.p, n * bits / 8, cudaMemcpyDeviceToHost, c->stream);
+      if (e != cudaSuccess) return e;
+      e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  c->caldata = calibrate(c, 1.1f, &e);
+  if (e != cudaSuccess) return e;
+
+  std::vector<float> Wh(c->nW);
+  e = cudaMemcpy(Wh.data(), c->W.p, c->nW * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  const int H = kHidden;
+  std::vector<float> W0pad((size_t)H * c->Fp, 0.0f);
+  for (int i = 0; i < H; i++) memcpy(&W0pad[(size_t)i * c->Fp], &Wh[(size_t)i * c->F], c->F * sizeof(float));
+  uint8_t* dec = c->decoder_host.data();
+  uint32_t* W0q = (uint32_t*)dec;
+  dec += H * c->Fp;
+  uint32_t* W1q = (uint32_t*)dec;
+  dec += H * H;
+  uint32_t* Woq = (uint32_t*)dec;
+  dec += kOutPad * H;
+  float* W0s = (float*)dec;
+  dec += H * sizeof(float);
+  float* W1s = (float*)dec;
+  dec += H * sizeof(float);
+  float* Wos = (float*)dec;
+  quantize_weights(W0pad.data(), H, c->Fp, 1.0f / 128.0f, W0q, W0s);
+  quantize_weights(&Wh[w1_off(c->F)], H, H, c->caldata.s_a1, W1q, W1s);
+  quantize_weights(&Wh[wo_off(c->F)], c->C, H, c->caldata.s_a2, Woq, Wos);
+  for (int i = c->C; i < kOutPad; i++) Wos[i] = 0.0f;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+ontc_context* ontc_create(void) { return new ontc_context(); }
+
+void ontc_destroy(ontc_context* c)
+{
+  if (!c) return;
+  unload(c);
+  if (c->h_steps) cudaFreeHost(c->h_steps);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int ontc_init(ontc_context* c, int32_t profile, void* stream)
+{
+  if (c->initialized) return ONTC_INVALID_STATE;
+  c->profile = profile;
+  switch (profile) {  // libopenntc.cpp:289-318
+    case ONTC_BPP_0_2: c->b0 = 2; c->b1 = 4; c->C0 = 8; c->C1 = 12; break;
+    case ONTC_BPP_0_5: c->b0 = 4; c->b1 = 4; c->C0 = 12; c->C1 = 20; break;
+    case ONTC_BPP_1_0: c->b0 = 2; c->b1 = 4; c->C0 = 12; c->C1 = 10; break;
+    case ONTC_BPP_2_25: c->b0 = 4; c->b1 = 4; c->C0 = 16; c->C1 = 12; break;
+    default: return ONTC_INVALID_STATE;
+  }
+  c->scale = (profile == ONTC_BPP_1_0 || profile == ONTC_BPP_2_25) ? 2 : 4;
+  c->d0 = 2.0f / powf(2.0f, (float)c->b0);
+  c->d1 = 2.0f / powf(2.0f, (float)c->b1);
+  c->F = round_up(4 * c->C0 + c->C1 + 12 + 1, 4);
+  c->Fp = round_up(c->F, 16);
+  c->nW = n_weights(c->F);
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return ONTC_CUDA_FAILURE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
+  c->max_grid = std::max(c->sms, std::max(1, tc_max_grid()));
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return ONTC_CUDA_FAILURE;
+    c->own_stream = true;
+  }
+  if (c->W.alloc(c->nW) || c->Wm.alloc(c->nW) || c->Wv.alloc(c->nW) || c->dWpart.alloc((size_t)c->max_grid * c->nW) ||
+      c->loss_part.alloc(c->max_grid) || c->calib.alloc(2) || c->eval_sums.alloc(ONTC_MAX_MIPS) ||
+      c->aux_steps.alloc(ONTC_MAX_MIPS) || c->tc_error.alloc(4) || !ensure_host_steps(c, 1024))
+    return ONTC_ALLOCATION_FAILURE;
+  cudaMemset(c->W.p, 0, c->nW * sizeof(float));
+  cudaMemset(c->tc_error.p, 0, 4 * sizeof(int));
+  const size_t dec = (size_t)kHidden * c->Fp + kHidden * kHidden + kOutPad * kHidden + kHidden * 4 + kHidden * 4 +
+                     kOutPad * 4;  // libopenntc.cpp:381-387
+  c->decoder_host.assign(dec, 0);
+  c->initialized = true;
+  return ONTC_SUCCESS;
+}
+
+int ontc_set_min_dimension(ontc_context* c, int32_t dim)
+{
+  if (dim < 16 || dim > ONTC_MAX_DIMENSION || std::popcount((unsigned)dim) != 1) return ONTC_INVALID_DIMENSION;
+  c->min_dimension = dim;
+  return ONTC_SUCCESS;
+}
+
+void ontc_unload_manifest(ontc_context* c) { unload(c); }
+
+int ontc_load_manifest(ontc_context* c, const char* path)
+{
+  unload(c);
+  if (!c->initialized) return ONTC_INVALID_STATE;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return ONTC_FILE_NOT_FOUND;
+  std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  Json j;
+  if (!Json::parse(text.data(), text.data() + text.size(), j) || !j.is_object() || !j.find("textures"))
+    return ONTC_INVALID_MANIFEST;
+  auto int_or = [](const Json& o, const char* k, int64_t d, bool& ok) -> int64_t {
+    const Json* v = o.find(k);
+    if (!v) return d;
+    if (!v->is_number()) {
+      ok = false;
+      return d;
+    }
+    return v->as_int();
+  };
+  bool ok = true;
+  const int64_t width = int_or(j, "width", -1, ok), height = int_or(j, "height", -1, ok);
+  if (!ok) return ONTC_INVALID_MANIFEST;
+  if (width == -1 && height == -1) return ONTC_INVALID_MANIFEST;
+  if (width != -1 && height != -1 && width != height) return ONTC_INVALID_MANIFEST;
+  const int64_t dim = width == -1 ? height : width;
+  if (dim < c->min_dimension || dim > ONTC_MAX_DIMENSION) return ONTC_INVALID_MANIFEST;
+
+  const Json& texs = *j.find("textures");
+  std::vector<const Json*> tlist;
+  if (texs.is_array()) {
+    for (const Json& t : texs.items()) tlist.push_back(&t);
+  } else if (texs.is_object()) {
+    for (const auto& kv : texs.members()) tlist.push_back(&kv.second);
+  } else {
+    tlist.push_back(&texs);
+  }
+  int count = 0;
+  for (const Json* t : tlist) {
+    const Json* sems = t->find("semantics");
+    const Json* fname = t->find("fileName");
+    if (!sems || !sems->is_object()) return ONTC_INVALID_MANIFEST;
+    if (!fname || !fname->is_string()) return ONTC_INVALID_MANIFEST;
+    for (const auto& kv : sems->members()) {  // key order, as nlohmann's std::map iterates
+      if (!kv.second.is_string()) return ONTC_INVALID_MANIFEST;
+      const int32_t sem = ontc_semantic_from_name(kv.first.c_str());
+      const std::string& chs = kv.second.as_string();
+      if (!valid_semantic_channels(sem, chs)) return ONTC_INVALID_MANIFEST;
+      if (count >= ONTC_MAX_SOURCES) return ONTC_INVALID_MANIFEST;
+      Source& s = c->sources[count];
+      s = Source();
+      s.path = fname->as_string();
+      const Json* nm = t->find("name");
+      if (nm && nm->is_string()) s.name = nm->as_string();
+      const Json* sr = t->find("isSRGB");
+      const Json* vf = t->find("verticalFlip");
+      if ((sr && !sr->is_bool()) || (vf && !vf->is_bool())) return ONTC_INVALID_MANIFEST;
+      s.srgb = sr ? sr->as_bool() : false;  // parsed but unused, as upstream (:1164)
+      s.vflip = vf ? vf->as_bool() : false;
+      s.sem = sem;
+      s.nch = ontc_channel_count_for_semantic(sem);
+      for (int i = 0; i < 4; i++) {
+        int ch = -1;
+        if (i < s.nch) ch = chs[i] == 'R' ? 0 : chs[i] == 'G' ? 1 : chs[i] == 'B' ? 2 : 3;
+        s.cmap[i] = ch;
+      }
+      count++;
+    }
+  }
+  c->source_count = count;
+  int total = 0;
+  for (int i = 0; i < count; i++) total += c->sources[i].nch;
+  if (total < 1 || total > ONTC_MAX_CHANNELS) return ONTC_INVALID_MANIFEST;
+  c->C = total;
+  std::stable_sort(c->sources, c->sources + count, [](const Source& a, const Source& b) { return a.sem < b.sem; });
+  if (dim < c->min_dimension || dim > ONTC_MAX_DIMENSION || std::popcount((unsigned)dim) != 1) return ONTC_INVALID_DIMENSION;
+
+  // mip and latent pyramids (libopenntc.cpp:1209-1227)
+  c->mip_dim[0] = (int)dim;
+  c->mips = 0;
+  while (c->mip_dim[c->mips] > 4) {
+    c->mip_dim[c->mips + 1] = c->mip_dim[c->mips] / 2;
+    c->mips++;
+  }
+  c->mips++;
+  c->levels = 0;
+  c->g0_dim[0] = c->mip_dim[0] / c->scale;
+  c->g1_dim[0] = c->g0_dim[0] / 2;
+  while (c->g0_dim[c->levels] / 4 >= 4) {
+    c->g0_dim[c->levels + 1] = c->g0_dim[c->levels] / 4;
+    c->g1_dim[c->levels + 1] = c->g1_dim[c->levels] / 4;
+    c->levels++;
+  }
+  c->levels++;
+
+  c->manifest_loaded = true;  // so that unload() releases partial allocations
+  auto fail = [&](int r) {
+    unload(c);
+    return r;
+  };
+  size_t words0 = 0, words1 = 0;
+  for (int l = 0; l < c->levels; l++) {
+    for (int g = 0; g < 2; g++) {
+      const size_t n = c->level_elems(g, l);
+      for (int k = 0; k < 4; k++)
+        if (c->lat[g][k][l].alloc(n) != cudaSuccess) return fail(ONTC_ALLOCATION_FAILURE);
+      cudaMemsetAsync(c->lat[g][3][l].p, 0, n * sizeof(float), c->stream);
+    }
+    words0 += c->level_elems(0, l) * c->b0 / 32;
+    words1 += c->level_elems(1, l) * c->b1 / 32;
+  }
+  if (c->packbuf.alloc(std::max(c->level_elems(0, 0) * c->b0 / 32, c->level_elems(1, 0) * c->b1 / 32) + 4))
+    return fail(ONTC_ALLOCATION_FAILURE);
+  c->g0_host_packed.assign(words0, 0);
+  c->g1_host_packed.assign(words1, 0);
+  size_t o0 = 0, o1 = 0;
+  for (int l = 0; l < c->levels; l++) {
+    c->g0_host[l] = c->g0_host_packed.data() + o0;
+    c->g1_host[l] = c->g1_host_packed.data() + o1;
+    o0 += c->level_elems(0, l) * c->b0 / 32;
+    o1 += c->level_elems(1, l) * c->b1 / 32;
+  }
+  for (int m = 0; m < c->mips; m++)
+    if (c->package[m].alloc((size_t)c->mip_dim[m] * c->mip_dim[m] * c->C)) return fail(ONTC_ALLOCATION_FAILURE);
+
+  // Mip chains per source (libopenntc.cpp:1296-1336)
+  const size_t n0 = (size_t)dim * dim;
+  DBuf<uint8_t> rgba_dev, chain[ONTC_MAX_MIPS];
+  DBuf<float> tmp;
+  std::vector<DBuf<uint8_t>> src_mips((size_t)count * c->mips);
+  if (rgba_dev.alloc(n0 * 4) || tmp.alloc(n0 * 2)) return fail(ONTC_ALLOCATION_FAILURE);
+  std::string base_dir;
+  {
+    std::string p(path);
+    const size_t sl = p.find_last_of('/');
+    if (sl != std::string::npos) base_dir = p.substr(0, sl + 1);
+  }
+  for (int i = 0; i < count; i++) {
+    const Source& s = c->sources[i];
+    std::vector<uint8_t> rgba;
+    int w = 0, h = 0;
+    bool loaded = load_image_rgba8(s.path, rgba, w, h);
+    // extension: relative paths that do not resolve from the working directory are
+    // also tried relative to the manifest's directory
+    if (!loaded && !s.path.empty() && s.path[0] != '/' && !base_dir.empty())
+      loaded = load_image_rgba8(base_dir + s.path, rgba, w, h);
+    if (!loaded) return fail(ONTC_FILE_NOT_FOUND);
+    if (w != h || w != dim) return fail(ONTC_INVALID_MANIFEST);
+    if (s.nch < 1) continue;  // a semantic with no channel count contributes no channels
+    if (cudaMemcpyAsync(rgba_dev.p, rgba.data(), n0 * 4, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+      return fail(ONTC_CUDA_FAILURE);
+    for (int m = 0; m < c->mips; m++)
+      if (src_mips[(size_t)i * c->mips + m].alloc((size_t)c->mip_dim[m] * c->mip_dim[m] * s.nch))
+        return fail(ONTC_ALLOCATION_FAILURE);
+    if (launch_prepare(rgba_dev.p, (int)dim, s.cmap, s.nch, src_mips[(size_t)i * c->mips].p, c->stream))
+      return fail(ONTC_CUDA_FAILURE);
+    c->launches++;
+    for (int m = 1; m < c->mips; m++) {
+      if (launch_lanczos_down(src_mips[(size_t)i * c->mips + m - 1].p, c->mip_dim[m - 1], s.nch, tmp.p,
+                              src_mips[(size_t)i * c->mips + m].p, c->stream))
+        return fail(ONTC_CUDA_FAILURE);
+      c->launches += 2;
+    }
+    for (int m = 0; m < c->mips; m++) {
+      c->mips_host[i][m].assign((size_t)c->mip_dim[m] * c->mip_dim[m] * s.nch, 0);
+      if (cudaMemcpyAsync(c->mips_host[i][m].data(), src_mips[(size_t)i * c->mips + m].p, c->mips_host[i][m].size(),
+                          cudaMemcpyDeviceToHost, c->stream))
+        return fail(ONTC_CUDA_FAILURE);
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(ONTC_CUDA_FAILURE);
+  }
+  // Channel interleave into the per-mip target package (libopenntc.cpp:1338-1362)
+  PackageSpec spec = {};
+  int p = 0;
+  for (int j2 = 0; j2 < count; j2++) {
+    spec.src_channels[j2] = c->sources[j2].nch;
+    for (int ch = 0; ch < c->sources[j2].nch; ch++) {
+      spec.feat_src[p] = j2;
+      spec.feat_chan[p] = ch;
+      p++;
+    }
+  }
+  if (p != c->C) return fail(ONTC_INVALID_MANIFEST);
+  for (int m = 0; m < c->mips; m++) {
+    for (int j2 = 0; j2 < count; j2++) spec.src[j2] = src_mips[(size_t)j2 * c->mips + m].p;
+    if (launch_package(spec, c->mip_dim[m], c->C, c->package[m].p, c->stream)) return fail(ONTC_CUDA_FAILURE);
+    c->launches++;
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(ONTC_CUDA_FAILURE);
+  c->train_phase = ONTC_MANIFEST_LOADED;
+  return ONTC_SUCCESS;
+}
+
+void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_batch)
+{
+  if (!c->manifest_loaded ||
+      (c->train_phase != ONTC_MANIFEST_LOADED && c->train_phase != ONTC_TRAIN_COMPLETE &&
+       c->train_phase != ONTC_TRAIN_IN_PROGRESS)) {
+    c->last_error = ONTC_INVALID_STATE;
+    return;
+  }
+  c->batch_count = ontc_steps_for_quality(quality);
+  c->lock_i = (95 * c->batch_count) / 100;
+  c->batch_i = 0;
+  c->grids = std::clamp(grids_per_batch, 1, kMaxGrids);
+  for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->grid_batch_i[l] = 0;
+  c->last_noise = false;
+
+  cudaError_t e = cudaSuccess;
+  std::vector<float> tmp;
+  std::uniform_real_distribution<float> lat(-0.1f, 0.1f);
+  for (int l = 0; l < c->levels; l++) {
+    for (int g = 0; g < 2; g++) {
+      const size_t n = c->level_elems(g, l);
+      tmp.resize(n);
+      for (size_t i = 0; i < n; i++) tmp[i] = lat(c->gen);
+      if (!e) e = cudaMemcpy(c->lat[g][0][l].p, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+      if (!e) e = cudaMemset(c->lat[g][1][l].p, 0, n * sizeof(float));
+      if (!e) e = cudaMemset(c->lat[g][2][l].p, 0, n * sizeof(float));
+      if (!e) e = cudaMemset(c->lat[g][3][l].p, 0, n * sizeof(float));
+    }
+  }
+  // Kaiming-uniform, bound 1/sqrt(fan_in) (libopenntc.cpp:60-78): W0 [64][F], W1 [64][64], Wout [16][64]
+  tmp.assign(c->nW, 0.0f);
+  auto kaiming = [&](float* dst, int rows, int cols) {
+    const float bound = 1.0f / sqrtf((float)cols);
+    std::uniform_real_distribution<float> d(-bound, bound);
+    for (int i = 0; i < rows * cols; i++) dst[i] = d(c->gen);
+  };
+  kaiming(&tmp[0], kHidden, c->F);
+  kaiming(&tmp[w1_off(c->F)], kHidden, kHidden);
+  kaiming(&tmp[wo_off(c->F)], kOutPad, kHidden);
+  if (!e) e = cudaMemcpy(c->W.p, tmp.data(), c->nW * sizeof(float), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemset(c->Wm.p, 0, c->nW * sizeof(float));
+  if (!e) e = cudaMemset(c->Wv.p, 0, c->nW * sizeof(float));
+  if (!e) e = c->losses.alloc((size_t)std::max(c->batch_count, 1));
+  if (!e) e = cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double));
+  if (e) c->last_error = ONTC_CUDA_FAILURE;
+  c->train_phase = ONTC_TRAIN_IN_PROGRESS;
+}
+
+int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
+{
+  if (!c->initialized || !o) return ONTC_INVALID_STATE;
+  if (o->precision != ONTC_PRECISION_FP32 && o->precision != ONTC_PRECISION_BF16) return ONTC_INVALID_STATE;
+  if (c->batch_i > 0) return ONTC_INVALID_STATE;
+  c->precision = o->precision;
+  if (o->steps_override > 0) {
+    c->batch_count = o->steps_override;
+    c->lock_i = (95 * c->batch_count) / 100;
+    if (c->manifest_loaded) {
+      if (c->losses.alloc((size_t)c->batch_count) || cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double)))
+        return ONTC_ALLOCATION_FAILURE;
+    }
+  }
+  if (o->has_lock_step) c->lock_i = std::max(0, o->lock_step);
+  return ONTC_SUCCESS;
+}
+
+// Context::Train (libopenntc.cpp:536-879)
+void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
+{
+  if (!c->manifest_loaded || (c->train_phase != ONTC_TRAIN_IN_PROGRESS && c->train_phase != ONTC_TRAIN_COMPLETE)) {
+    *out = make_progress(ONTC_TRAIN_ERROR, ONTC_INVALID_STATE, c);
+    return;
+  }
+  if (num_batches < 0) num_batches = 0;
+  const int remaining = std::max(0, c->batch_count - c->batch_i);
+  const int n = std::min(remaining, num_batches);
+  const int target = c->batch_i + n;
+  if (c->batch_i == target) {
+    *out = make_progress(ONTC_TRAIN_COMPLETE, ONTC_SUCCESS, c);
+    return;
+  }
+  std::bernoulli_distribution dist_batch_type(0.05);
+  std::uniform_real_distribution<float> dist_u(0.0f, 1.0f);
+  std::uniform_int_distribution<int> dist_lod(0, c->mips - 1);
+  const Model M = c->model();
+  const int chunk_cap = 1024;
+  if (!ensure_host_steps(c, chunk_cap) || (c->steps.n < (size_t)chunk_cap && c->steps.alloc(chunk_cap))) {
+    c->last_error = ONTC_CUDA_FAILURE;
+    *out = make_progress(ONTC_TRAIN_ERROR, ONTC_CUDA_FAILURE, c);
+    return;
+  }
+  cudaError_t e = cudaSuccess;
+  while (c->batch_i < target && e == cudaSuccess) {
+    // The previous chunk's kernels may still read the staging and device records.
+    e = cudaStreamSynchronize(c->stream);
+    if (e) break;
+    const int first = c->batch_i;
+    int cnt = std::min(chunk_cap, target - first);
+    // a chunk ends at the lock step so the latents can be snapped before it runs
+    if (first < c->lock_i && first + cnt > c->lock_i) cnt = c->lock_i - first;
+    for (int k = 0; k < cnt; k++) {
+      const int bi = first + k;
+      const bool draw_uniform = dist_batch_type(c->gen);
+      const float U = dist_u(c->gen);
+      const float fl = std::floor(0.5f * -std::log2(U));
+      int lod = (fl < 1e9f) ? std::min((int)fl, c->mips - 1) : c->mips - 1;
+      const int lod_uniform = dist_lod(c->gen);
+      if (draw_uniform) lod = lod_uniform;
+      StepRec& s = c->h_steps[k];
+      s = StepRec();
+      s.lod = lod;
+      s.level = c->feature_level_for_lod(lod);
+      s.mip_dim = c->mip_dim[lod];
+      std::uniform_int_distribution<int> dist_grid(0, c->mip_dim[lod] - 1);
+      for (int g = 0; g < c->grids; g++) {
+        s.ox[g] = dist_grid(c->gen);
+        s.oy[g] = dist_grid(c->gen);
+      }
+      s.tile_dim = std::min(c->mip_dim[lod], 256);
+      s.n_grids = c->grids;
+      s.texels = c->grids * s.tile_dim * s.tile_dim;
+      s.noise = bi < c->lock_i ? 1 : 0;
+      s.grid_update = bi < c->lock_i ? 1 : 0;
+      s.seed = step_seed((uint32_t)bi);
+      s.norm_lod = lod / static_cast<float>(c->mips - 1);
+      s.b1 = 1.0f / (1.0f - powf(0.9f, bi + 1.0f));
+      s.b2 = 1.0f / (1.0f - powf(0.999f, bi + 1.0f));
+      s.gb1 = 1.0f / (1.0f - powf(0.9f, c->grid_batch_i[s.level] + 1.0f));
+      s.gb2 = 1.0f / (1.0f - powf(0.999f, c->grid_batch_i[s.level] + 1.0f));
+      c->grid_batch_i[s.level] += 1;
+      s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
+      s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
+      s.step = bi;
+    }
+    e = cudaMemcpyAsync(c->steps.p, c->h_steps, cnt * sizeof(StepRec), cudaMemcpyHostToDevice, c->stream);
+    for (int k = 0; k < cnt && e == cudaSuccess; k++) {
+      const int bi = first + k;
+      const StepRec& s = c->h_steps[k];
+      if (bi == c->lock_i) {
+        // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
+        for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
+          e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
+          if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
+          c->launches += 2;
+        }
+      }
+      const int units = (s.texels + kTile - 1) / kTile;
+      TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
+      int grid = std::min(units, c->sms);
+      if (c->precision == ONTC_PRECISION_BF16) {
+        grid = std::min(units, tc_max_grid());
+        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
+        if (e == cudaErrorNotSupported) {
+          cudaGetLastError();
+          grid = std::min(units, c->sms);
+          e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+        }
+      } else {
+        e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+      }
+      c->launches++;
+      if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
+      c->launches++;
+      c->last_seed = s.seed;
+      c->last_noise = s.noise != 0;
+      c->batch_i = bi + 1;
+    }
+  }
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    c->last_error = ONTC_CUDA_FAILURE;
+    *out = make_progress(ONTC_TRAIN_ERROR, ONTC_CUDA_FAILURE, c);
+    return;
+  }
+  *out = make_progress(ONTC_TRAIN_IN_PROGRESS, ONTC_SUCCESS, c);
+  if (c->batch_i == c->batch_count) {
+    out->phase = ONTC_TRAIN_COMPLETE;
+    c->train_phase = ONTC_TRAIN_COMPLETE;
+    if (complete_training(c) != cudaSuccess) {
+      c->last_error = ONTC_CUDA_FAILURE;
+      *out = make_progress(ONTC_TRAIN_ERROR, ONTC_CUDA_FAILURE, c);
+    }
+  }
+}
+
+void ontc_train_until_complete(ontc_context* c, ontc_train_progress* out) { ontc_train(c, c->batch_count, out); }
+
+void ontc_eval(ontc_context* c, ontc_eval_results* out)
+{
+  *out = ontc_eval_results{};
+  if (!c->manifest_loaded || (c->train_phase != ONTC_TRAIN_IN_PROGRESS && c->train_phase != ONTC_TRAIN_COMPLETE)) {
+    c->last_error = ONTC_INVALID_STATE;
+    return;
+  }
+  std::vector<double> sums;
+  if (full_forward(c, kEval, &sums) != cudaSuccess) {
+    c->last_error = ONTC_CUDA_FAILURE;
+    return;
+  }
+  double num = 0.0, den = 0.0;
+  for (int m = 0; m < c->mips; m++) {
+    num += sums[m];
+    den += (double)c->mip_dim[m] * c->mip_dim[m] * c->C;
+  }
+  out->mse = num / den;
+  out->psnr = -10.0 * std::log10(out->mse);
+}
+
+void ontc_calibrate(ontc_context* c, float headroom, ontc_calibration* out)
+{
+  *out = ontc_calibration{};
+  if (!c->manifest_loaded || c->train_phase != ONTC_TRAIN_COMPLETE) {
+    c->last_error = ONTC_INVALID_STATE;
+    return;
+  }
+  cudaError_t e;
+  *out = calibrate(c, headroom, &e);
+  if (e != cudaSuccess) {
+    c->last_error = ONTC_CUDA_FAILURE;
+    *out = ontc_calibration{};
+  }
+}
+
+void ontc_get_compressed_data(ontc_context* c, ontc_compressed_data* d)
+{
+  memset(d, 0, sizeof(*d));
+  if (!c->manifest_loaded) return;
+  for (int i = 0; i < c->levels; i++) {
+    d->g0[i] = c->g0_host[i];
+    d->g0_size[i] = c->level_elems(0, i) * c->b0 / 8;
+    d->g1[i] = c->g1_host[i];
+    d->g1_size[i] = c->level_elems(1, i) * c->b1 / 8;
+  }
+  for (int i = 1; i < c->levels; i++) {
+    d->g0_offset[i] = d->g0_offset[i - 1] + d->g0_size[i - 1];
+    d->g1_offset[i] = d->g1_offset[i - 1] + d->g1_size[i - 1];
+  }
+  d->g0_total_size = d->g0_offset[c->levels - 1] + d->g0_size[c->levels - 1];
+  d->g1_total_size = d->g1_offset[c->levels - 1] + d->g1_size[c->levels - 1];
+  d->decoder = c->decoder_host.data();
+  d->decoder_size = c->decoder_host.size();
+  for (int i = 0; i < c->levels; i++) {
+    d->g0_grid_dim[i] = c->g0_dim[i];
+    d->g1_grid_dim[i] = c->g1_dim[i];
+  }
+  d->profile = c->profile;
+  d->g0_bits_per_channel = c->b0;
+  d->g1_bits_per_channel = c->b1;
+  d->g0_channels = c->C0;
+  d->g1_channels = c->C1;
+  d->dim = c->mip_dim[0];
+  d->mip_count = c->mips;
+  d->level_count = c->levels;
+  d->caldata = c->caldata;
+  d->channel_count = 0;
+  for (int i = 0; i < c->source_count; i++)
+    for (int k = 0; k < c->sources[i].nch && d->channel_count < ONTC_MAX_CHANNELS; k++)
+      d->channel_semantics[d->channel_count++] = c->sources[i].sem;
+}
+
+void ontc_get_texture_data(ontc_context* c, ontc_texture_data* t)
+{
+  memset(t, 0, sizeof(*t));
+  if (!c->manifest_loaded) return;
+  t->tex_count = c->source_count;
+  t->mip_count = c->mips;
+  for (int i = 0; i < c->source_count; i++) {
+    t->semantics[i] = c->sources[i].sem;
+    t->channels[i] = c->sources[i].nch;
+    for (int m = 0; m < c->mips; m++) t->mips[i][m] = c->mips_host[i][m].empty() ? nullptr : c->mips_host[i][m].data();
+  }
+}
+
+int32_t ontc_get_mip_dim(ontc_context* c, int32_t mip)
+{
+  if (c->initialized && c->manifest_loaded && mip >= 0 && mip < c->mips) return c->mip_dim[mip];
+  return 0;
+}
+
+int32_t ontc_feature_level_for_lod(ontc_context* c, int32_t lod) { return c->feature_level_for_lod(lod); }
+
+int ontc_get_last_error(ontc_context* c) { return c->last_error; }
+
+int32_t ontc_steps_for_quality(int32_t q)
+{
+  switch (q) {  // libopenntc.cpp:428-443
+    case ONTC_QUALITY_LOW: return 30000;
+    case ONTC_QUALITY_MEDIUM: return 120000;
+    case ONTC_QUALITY_HIGH: return 240000;
+    case ONTC_QUALITY_ULTRA: return 480000;
+    default: return 30000;
+  }
+}
+
+int ontc_get_step_losses(ontc_context* c, double* out, int32_t n)
+{
+  if (!c->manifest_loaded || !c->losses.p || n <= 0) return ONTC_INVALID_STATE;
+  n = std::min(n, c->batch_i);
+  if (n == 0) return ONTC_SUCCESS;
+  if (cudaMemcpy(out, c->losses.p + (c->batch_i - n), n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return ONTC_CUDA_FAILURE;
+  return ONTC_SUCCESS;
+}
+
+int64_t ontc_kernel_launch_count(ontc_context* c) { return c->launches; }
+
+const char* ontc_version(void) { return "ontc 0.1 sm_100a"; }
+
+}  // extern "C"

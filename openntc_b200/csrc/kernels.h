@@ -1,0 +1,59 @@
+// Host-side launchers of libontc's kernels (all on the caller's stream, all unchecked
+// for work errors but checked for launch errors).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ontc {
+
+enum { kTrain = 0, kEval = 1, kCalib = 2 };
+
+struct TileOut {
+  float* dW_partial;     // [grid][nW] per-CTA decoder gradient partial sums (kTrain)
+  double* loss_partial;  // [grid] per-CTA sum of squared residuals (kTrain, kEval)
+  float* calib_max;      // [2] running max |a0|, |a1| as ordered ints (kCalib)
+};
+
+// ---- training / eval units
+size_t simt_smem_bytes(int F);
+cudaError_t launch_simt_units(int mode, const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
+                              cudaStream_t stream);
+// BF16 tcgen05 path; returns cudaErrorNotSupported when the profile has no tcgen05 variant
+cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
+                            int* d_error, cudaStream_t stream);
+int tc_max_grid();
+
+// ---- optimiser: decoder Adam (reducing `grid` partials) + dense latent Adam/clamp/zero
+// of the step's level, one launch.  Also reduces the loss partials into loss_out[step].
+cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, const float* dW_partial,
+                             const double* loss_partial, int grid, double* loss_out, cudaStream_t stream);
+// upstream quantize_grid over one latent tensor (ntc_kernel.cu:448-460)
+cudaError_t launch_quantize_grid(float* g, long long n, int bits, float delta, cudaStream_t stream);
+// upstream quantize_pack (ntc_kernel.cu:486-499), n*bits must be a multiple of 32
+cudaError_t launch_quantize_pack(const float* in, long long n, int bits, uint32_t* out, cudaStream_t stream);
+// fills n floats with v
+cudaError_t launch_fill(float* p, long long n, float v, cudaStream_t stream);
+// out = sum over the first n doubles (single CTA, deterministic order)
+cudaError_t launch_sum_doubles(const double* in, int n, double* out, cudaStream_t stream);
+
+// ---- mip chain (LoadManifest)
+// picks `cmap_count` channels (cmap[i] in 0..3) out of an RGBA8 image into [dim][dim][count]
+cudaError_t launch_prepare(const uint8_t* rgba, int dim, const int* cmap, int count, uint8_t* out, cudaStream_t stream);
+// one separable Lanczos-3 2x reduction [dim][dim][c] -> [dim/2][dim/2][c]; tmp holds dim*dim/2*c floats
+cudaError_t launch_lanczos_down(const uint8_t* src, int dim, int c, float* tmp, uint8_t* dst, cudaStream_t stream);
+// interleaves the sources' channels into the [dim][dim][C] target package
+struct PackageSpec {
+  const uint8_t* src[16];
+  int32_t src_channels[16];
+  int32_t feat_src[16];
+  int32_t feat_chan[16];
+};
+cudaError_t launch_package(const PackageSpec& spec, int dim, int C, uint8_t* out, cudaStream_t stream);
+// the 12 Lanczos-3 tap weights as the filter computes them (test hook)
+cudaError_t lanczos_weights(float* host12);
+
+}  // namespace ontc
