@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Training-throughput benchmark: train samples/s on one B200 per rank.
+
+Workload (the mixed-precision-at-scale configuration): a seeded 2048x2048 9-channel
+synthetic PBR set, profile Bpp_1_0, 4 tiles of 256x256 texels per step (262,144 samples),
+a 10,000-step schedule (latent lock at step 9,500), BF16 MLP with fp32 master weights and
+moments.  A "step" is one optimisation step: draw -> gather -> MLP forward/backward ->
+latent scatter -> Adam over the whole current latent level.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision bf16|fp32]
+
+Prints one JSON line (rank 0).  `value` is device-timed with CUDA events on the library's
+stream (max over ranks); `e2e` is the same steps through the C ABI timed on the host,
+including the per-step draw upload and the read-back of every step's loss.
+--impl reference times upstream's own Context::Train built from its sources (oracle/_ref).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = {
+    "workload": "train_2048sq_9ch_bpp1_0_b262144",
+    "dim": 2048, "channels": 9, "profile": "Bpp_1_0", "profile_id": 2, "grids_per_batch": 4,
+    "batch_texels": 4 * 256 * 256, "schedule_steps": 10000, "seed": 1,
+}
+METRIC = "train samples/s"
+L2_NOTE = ("inputs larger than L2: each step streams the whole level-0 latent set "
+           "(15.2M latents x 16 B of p/m/v/g = 243 MB > 126 MB L2)")
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "src": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(float(r[2]) for r in rows), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_set(base: Path, seed: int) -> Path:
+    from openntc_b200.synth import make_material
+    return make_material(base / f"set_{seed}", WORKLOAD["dim"], seed, WORKLOAD["channels"])
+
+
+def cpu_baseline(manifest: Path, budget_s: float = 12.0):
+    """The oracle's fp64 training step on the host cores, on a bounded sample: one 256x256
+    tile per step (65,536 samples) plus the dense latent Adam over level 0, repeated until
+    `budget_s` of work."""
+    import numpy as np
+    import openntc_b200 as ont
+    from oracle.bindings import Oracle
+    from tests import helpers as H
+
+    threads = os.cpu_count() or 1
+    oracle = Oracle()
+    ctx = H.new_context(WORKLOAD["profile_id"], manifest, min_dim=16, grids=1, steps=WORKLOAD["schedule_steps"],
+                        precision=ont.Precision.FP32)
+    ctx.train(1)
+    s = H.last_step(ctx)
+    m, level = H.oracle_model(oracle, ctx, WORKLOAD["profile_id"], 0)
+    sh = H.shape(ctx)
+    b0, b1, *_ = H.PROFILE_SHAPES[WORKLOAD["profile_id"]]
+    p0 = H.tensor(ctx, 0, 0)
+    p1 = H.tensor(ctx, 1, 0)
+    st = oracle.step(256, [(s.ox[0], s.oy[0])], 1, s.seed, 0.0)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        _, dW, dG0, dG1 = oracle.step_gradients(m, st, threads=threads)
+        for p, g, bits in ((p0, dG0, b0), (p1, dG1, b1)):
+            z = np.zeros_like(p)
+            oracle.adam(p, z, z.copy(), g.astype(np.float32), 1e-3, 1.0, 1.0, 1, 2.0 / 2 ** bits)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 50:
+            break
+    ctx.destroy()
+    samples = n * 256 * 256
+    return {"value": samples / el, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{n} oracle steps (fp64 MLP fwd/bwd over one 256x256 tile of the workload + fp32 dense "
+                      f"latent Adam over level 0, {sh['g0'][0]}^2x{m.C0} + {sh['g1'][0]}^2x{m.C1} latents), "
+                      f"{el:.1f} s on {threads} host threads"}
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    import openntc_b200 as ont
+    from openntc_b200 import _abi
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    tmp = Path(tempfile.mkdtemp(prefix=f"ontc_bench_{rank}_"))
+    manifest = make_set(tmp, WORKLOAD["seed"] + rank)  # weak scaling: one material per rank
+    stream = torch.cuda.Stream()
+    ctx = ont.Context()
+    r = ctx.init(WORKLOAD["profile_id"], stream.cuda_stream)
+    assert r == ont.Result.Success, r
+    assert ctx.load_manifest(manifest) == ont.Result.Success
+    precision = ont.Precision.BF16 if args.precision == "bf16" else ont.Precision.FP32
+    ctx.begin_training(ont.Quality.Low, WORKLOAD["grids_per_batch"], steps=WORKLOAD["schedule_steps"],
+                       precision=precision)
+    K, W = args.steps, args.warmup
+    assert W + 3 * K + 1 < int(0.95 * WORKLOAD["schedule_steps"]), "timed steps must stay before the latent lock"
+    B = WORKLOAD["batch_texels"]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p = ctx.train(W)
+    assert p.result == 0, p
+
+    # ---- value: K steps, device-timed on the library's stream
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.kernel_launches()
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        p = ctx.train(K)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    assert p.result == 0, p
+    launches = ctx.kernel_launches() - l0
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    clocks = clk.summary()
+    value = world * K * B / (ms / 1e3)
+
+    # ---- e2e: K steps through the C ABI, host-timed: draws uploaded and every step's loss read back
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    p = ctx.train(K)
+    losses = ctx.step_losses(K)
+    t1 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(t1 - t0)
+    assert p.result == 0 and all(l > 0 for l in losses)
+
+    # ---- roofline of the dominant kernel: per-launch CUDA events on the same stream
+    ctx._lib.ontc_profile_kernels(ctx.handle, 1)
+    ctx.train(K)
+    kt = (_abi.KernelTime * _abi.KCLASS_COUNT)()
+    ctx._lib.ontc_kernel_times(ctx.handle, kt, _abi.KCLASS_COUNT)
+    ctx._lib.ontc_profile_kernels(ctx.handle, 0)
+    pk = peaks()
+    adam = kt[_abi.KCLASS_ADAM]
+    units = kt[_abi.KCLASS_UNITS_BF16 if precision == ont.Precision.BF16 else _abi.KCLASS_UNITS_FP32]
+    if units.launches == 0:
+        units = kt[_abi.KCLASS_UNITS_FP32]
+    step_ms_prof = (adam.total_ms + units.total_ms) / max(1, adam.launches)
+    adam_gbs = adam.bytes / (adam.total_ms / 1e3) / 1e9 if adam.total_ms > 0 else 0.0
+    units_tflops = units.flops / (units.total_ms / 1e3) / 1e12 if units.total_ms > 0 else 0.0
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("adam_step_bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": "adam_step_kernel (fused latent Adam/clamp/zero + decoder Adam)",
+                "achieved": round(adam_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(adam_gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"],
+                "traffic": traffic, "algorithmic_bytes_per_launch": adam.bytes / max(1, adam.launches),
+                "avg_launch_us": 1e3 * adam.total_ms / max(1, adam.launches),
+                "share_of_step": round(adam.total_ms / max(1e-9, adam.total_ms + units.total_ms), 3),
+                "mlp_kernel": {"name": "fused tile kernel (gather/MLP fwd+bwd/scatter)",
+                               "achieved_tflops": round(units_tflops, 2), "peak_tflops": pk["bf16_tflops"],
+                               "frac": round(units_tflops / pk["bf16_tflops"], 4),
+                               "avg_launch_us": 1e3 * units.total_ms / max(1, units.launches)}}
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(manifest)
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": "samples/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic: seeded 2048^2 9-channel PBR set (value-noise height, ramp albedo, normals, "
+                    "roughness, metallic, AO), one material per rank",
+            "config": dict(WORKLOAD, precision=args.precision, l2=L2_NOTE,
+                           parallelism=f"replicas x{world} (independent materials, no collective)"),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(world * K * B / e2e_s, 1), "unit": "samples/s",
+                    "h2d_bytes_per_step": 128, "d2h_bytes_per_step": 8,
+                    "what": "ontc_train(K) + ontc_get_step_losses(K) through the C ABI, host wall clock"},
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "impl": "ours",
+            "profiled_ms_per_step": round(step_ms_prof, 4),
+        }
+        print(json.dumps(out), flush=True)
+    ctx.destroy()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return None
+    from oracle.bindings import REF_SO, RefContext
+    if not REF_SO.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"{REF_SO.relative_to(ROOT)} not built"}))
+        return None
+    import ctypes as C
+    try:
+        C.CDLL("libcudart.so.12")
+    except OSError:
+        pass
+    tmp = Path(tempfile.mkdtemp(prefix="ontc_bench_ref_"))
+    manifest = make_set(tmp, WORKLOAD["seed"])
+    ref = RefContext(WORKLOAD["profile_id"])
+    assert ref.init_result == 0, ref.init_result
+    assert ref.load_manifest(manifest) == 0
+    ref.begin_training(0, WORKLOAD["grids_per_batch"], WORKLOAD["schedule_steps"], -1)
+    K, W = args.steps, args.warmup
+    ref.train(W)
+    with Clocks(local) as clk:
+        ms, prog, err = ref.time_train(K)
+    assert err == 0 and prog[1] == 0, (err, prog)
+    B = WORKLOAD["batch_texels"]
+    value = K * B / (ms / 1e3)
+    t0 = time.perf_counter()
+    ref.train(K)
+    e2e_s = time.perf_counter() - t0
+    ref.close()
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "samples/s", "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 (cuBLAS TF32 GEMMs)", "data": "synthetic: same seeded 2048^2 9-channel PBR set",
+        "config": dict(WORKLOAD, precision="upstream"), "impl": "reference",
+        "cpu_baseline": {"value": round(value, 1), "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"upstream Context::Train built from its own sources (cuBLAS TF32 + its CUDA "
+                                   f"kernels; upstream has no CPU training path), {K} steps on the GPU"},
+        "e2e": {"value": round(K * B / e2e_s, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -223,10 +223,28 @@ const char* ontc_semantic_to_string(int32_t semantic);
 int32_t ontc_semantic_from_name(const char* name);
 int32_t ontc_channel_count_for_semantic(int32_t semantic);
 
-/* ---- Library facts --------------------------------------------------------------------- */
+/* ---- Library facts and kernel timing (no upstream counterpart) ------------------------- */
 
 /* Number of kernel launches this context issued so far (all of them are libontc's own). */
 int64_t ontc_kernel_launch_count(ontc_context* ctx);
+
+/* Kernel classes timed by ontc_profile_kernels. */
+enum {
+  ONTC_KCLASS_UNITS_FP32 = 0, /* fused gather/MLP/backward/scatter tile kernel, fp32 SIMT */
+  ONTC_KCLASS_UNITS_BF16 = 1, /* the same, tcgen05 bf16 */
+  ONTC_KCLASS_ADAM = 2,       /* fused decoder + latent Adam / clamp / gradient-zero pass */
+  ONTC_KCLASS_COUNT = 3
+};
+typedef struct ontc_kernel_time {
+  int64_t launches;
+  double total_ms; /* sum of CUDA-event durations on the context's stream */
+  double bytes;    /* algorithmic DRAM bytes of those launches */
+  double flops;    /* algorithmic flops of those launches */
+} ontc_kernel_time;
+/* Enables (1) or disables (0) event timing of every training-step launch and clears the record. */
+int ontc_profile_kernels(ontc_context* ctx, int32_t enable);
+/* Totals per class since the last ontc_profile_kernels; returns the number of classes written. */
+int ontc_kernel_times(ontc_context* ctx, ontc_kernel_time* out, int32_t max_classes);
 /* Version string of the build ("ontc <git-describe> sm_100a"). */
 const char* ontc_version(void);
 

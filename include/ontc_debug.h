@@ -1,0 +1,81 @@
+/*
+ * ontc_debug.h -- introspection entry points of libontc.so for tests and tools.
+ *
+ * No upstream counterpart: upstream keeps these tensors private (libopenntc.h:256-322).
+ * They let a checker read or overwrite the training state, replay one step's gradient
+ * computation for a chosen draw without the optimiser update, and run the bit-exact
+ * kernels (latent packing, mip reduction) on arbitrary inputs.
+ */
+#ifndef ONTC_DEBUG_H_
+#define ONTC_DEBUG_H_
+
+#include "ontc.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Tensor selectors for ontc_debug_tensor. */
+enum {
+  ONTC_DBG_G0 = 0,      /* latents g0[level], fp32 [dim][dim][C0] */
+  ONTC_DBG_G1 = 1,      /* latents g1[level] */
+  ONTC_DBG_G0_M = 2,    /* Adam first moment of g0[level] */
+  ONTC_DBG_G0_V = 3,
+  ONTC_DBG_G1_M = 4,
+  ONTC_DBG_G1_V = 5,
+  ONTC_DBG_G0_GRAD = 6, /* latent gradient buffers (zero between steps) */
+  ONTC_DBG_G1_GRAD = 7,
+  ONTC_DBG_W = 10,      /* decoder, fp32: W0 [64][F] | W1 [64][64] | Wout [16][64] */
+  ONTC_DBG_W_M = 11,
+  ONTC_DBG_W_V = 12,
+  ONTC_DBG_W_GRAD = 13  /* read-only: decoder gradient of the last ontc_debug_gradients call */
+};
+
+/* One step's draw (upstream's lod and tile origins, libopenntc.cpp:564-583). */
+typedef struct ontc_debug_step {
+  int32_t lod;
+  int32_t n_grids;
+  int32_t ox[8];
+  int32_t oy[8];
+  int32_t noise;  /* nonzero: add the quantisation-noise surrogate with stream `seed` */
+  uint32_t seed;
+  int32_t step;   /* global step index the draw belongs to */
+  int32_t level;  /* feature level (filled in by the library) */
+  /* schedule of that step (libopenntc.cpp:711-720), reported by ontc_debug_last_step */
+  float lr_grid, lr_dec, b1, b2, gb1, gb2;
+  int32_t grid_update;
+  int32_t pad;
+} ontc_debug_step;
+
+/* Copies between a state tensor and host memory (to_device = 0: device -> host).
+ * n <= 0 returns the element count without copying.  Returns the count or -1. */
+int64_t ontc_debug_tensor(ontc_context* ctx, int32_t which, int32_t level, float* host, int64_t n, int32_t to_device);
+
+/* The draw of the most recent training step. */
+int ontc_debug_last_step(ontc_context* ctx, ontc_debug_step* out);
+
+/* Gradient of the step loss for `step` at the current state: zeroes the step level's
+ * latent gradients, runs the training tile kernel of the context's precision and leaves
+ * the latent gradients in ONTC_DBG_G*_GRAD and the decoder gradient in ONTC_DBG_W_GRAD.
+ * Writes the mean squared residual to *loss.  Parameters are not updated. */
+int ontc_debug_gradients(ontc_context* ctx, ontc_debug_step* step, double* loss);
+
+/* Upstream quantize_pack on host floats through libontc's kernel (n * bits % 32 == 0). */
+int ontc_debug_quantize_pack(const float* host_in, int64_t n, int32_t bits, uint32_t* host_out);
+
+/* One Lanczos-3 2x reduction of a host [dim][dim][c] u8 image through libontc's kernels. */
+int ontc_debug_lanczos_down(const uint8_t* src, int32_t dim, int32_t c, uint8_t* dst);
+
+/* The 12 tap weights the reduction uses, as evaluated on the device. */
+int ontc_debug_lanczos_weights(float* out12);
+
+/* The interleaved u8 target package of one mip, [dim][dim][C]. */
+int ontc_debug_package(ontc_context* ctx, int32_t mip, uint8_t* out);
+
+/* Geometry: [F, Fp, C, mips, levels, nW, g0_dim[6], g1_dim[6], mip_dim[12], batch_i, lock_i, batch_count] */
+int ontc_debug_shape(ontc_context* ctx, int32_t* out32);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ONTC_DEBUG_H_ */

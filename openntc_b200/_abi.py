@@ -80,7 +80,24 @@ class TrainOptions(C.Structure):
                 ("precision", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
-# name -> (restype, argtypes); every symbol include/ontc.h declares.
+class KernelTime(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("total_ms", C.c_double), ("bytes", C.c_double), ("flops", C.c_double)]
+
+
+KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_COUNT = 0, 1, 2, 3
+
+
+class DebugStep(C.Structure):
+    _fields_ = [("lod", C.c_int32), ("n_grids", C.c_int32), ("ox", C.c_int32 * 8), ("oy", C.c_int32 * 8),
+                ("noise", C.c_int32), ("seed", C.c_uint32), ("step", C.c_int32), ("level", C.c_int32),
+                ("lr_grid", C.c_float), ("lr_dec", C.c_float), ("b1", C.c_float), ("b2", C.c_float),
+                ("gb1", C.c_float), ("gb2", C.c_float), ("grid_update", C.c_int32), ("pad", C.c_int32)]
+
+
+DBG_G0, DBG_G1, DBG_G0_M, DBG_G0_V, DBG_G1_M, DBG_G1_V, DBG_G0_GRAD, DBG_G1_GRAD = range(8)
+DBG_W, DBG_W_M, DBG_W_V, DBG_W_GRAD = 10, 11, 12, 13
+
+# name -> (restype, argtypes); every symbol include/ontc.h and include/ontc_debug.h declare.
 P = C.c_void_p
 SIGNATURES = {
     "ontc_create": (P, []),
@@ -113,6 +130,16 @@ SIGNATURES = {
     "ontc_channel_count_for_semantic": (C.c_int32, [C.c_int32]),
     "ontc_kernel_launch_count": (C.c_int64, [P]),
     "ontc_version": (C.c_char_p, []),
+    "ontc_profile_kernels": (C.c_int, [P, C.c_int32]),
+    "ontc_kernel_times": (C.c_int, [P, C.POINTER(KernelTime), C.c_int32]),
+    "ontc_debug_tensor": (C.c_int64, [P, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),
+    "ontc_debug_last_step": (C.c_int, [P, C.POINTER(DebugStep)]),
+    "ontc_debug_gradients": (C.c_int, [P, C.POINTER(DebugStep), C.POINTER(C.c_double)]),
+    "ontc_debug_quantize_pack": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "ontc_debug_lanczos_down": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "ontc_debug_lanczos_weights": (C.c_int, [C.c_void_p]),
+    "ontc_debug_package": (C.c_int, [P, C.c_int32, C.c_void_p]),
+    "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
 }
 
 

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ontc.h"
+#include "../../include/ontc_debug.h"
 #include "image.h"
 #include "json.h"
 #include "kernels.h"
@@ -174,6 +175,45 @@ struct ontc_context {
   std::vector<uint8_t> mips_host[ONTC_MAX_SOURCES][ONTC_MAX_MIPS];
 
   int64_t launches = 0;
+  StepRec last_step = {};
+
+  // optional per-kernel timing (ontc_profile_kernels): CUDA events around each launch on
+  // the context's stream, reduced when ontc_kernel_times is called
+  struct ProfRec {
+    int cls;
+    cudaEvent_t a, b;
+    double bytes, flops;
+  };
+  bool profiling = false;
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> event_pool;
+  cudaEvent_t prof_a = nullptr;
+  cudaEvent_t get_event()
+  {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void prof_begin()
+  {
+    if (!profiling) return;
+    prof_a = get_event();
+    cudaEventRecord(prof_a, stream);
+  }
+  void prof_end(int cls, double bytes, double flops)
+  {
+    if (!profiling || !prof_a) return;
+    cudaEvent_t b = get_event();
+    cudaEventRecord(b, stream);
+    prof.push_back({cls, prof_a, b, bytes, flops});
+    prof_a = nullptr;
+  }
+  std::vector<float> last_dW;  // decoder gradient of the last ontc_debug_gradients
 
   Model model() const
   {
@@ -445,7 +485,6 @@ void ontc_unload_manifest(ontc_context* c) { unload(c); }
 int ontc_load_manifest(ontc_context* c, const char* path)
 {
   unload(c);
-  if (!c->initialized) return ONTC_INVALID_STATE;
   std::ifstream f(path, std::ios::binary);
   if (!f) return ONTC_FILE_NOT_FOUND;
   std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
@@ -517,6 +556,8 @@ int ontc_load_manifest(ontc_context* c, const char* path)
   c->C = total;
   std::stable_sort(c->sources, c->sources + count, [](const Source& a, const Source& b) { return a.sem < b.sem; });
   if (dim < c->min_dimension || dim > ONTC_MAX_DIMENSION || std::popcount((unsigned)dim) != 1) return ONTC_INVALID_DIMENSION;
+  // manifest validation above needs no device; everything below does
+  if (!c->initialized) return ONTC_INVALID_STATE;
 
   // mip and latent pyramids (libopenntc.cpp:1209-1227)
   c->mip_dim[0] = (int)dim;
@@ -783,22 +824,33 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       const int units = (s.texels + kTile - 1) / kTile;
       TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
       int grid = std::min(units, c->sms);
+      int cls = ONTC_KCLASS_UNITS_FP32;
+      c->prof_begin();
       if (c->precision == ONTC_PRECISION_BF16) {
         grid = std::min(units, tc_max_grid());
+        cls = ONTC_KCLASS_UNITS_BF16;
         e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
         if (e == cudaErrorNotSupported) {
           cudaGetLastError();
           grid = std::min(units, c->sms);
+          cls = ONTC_KCLASS_UNITS_FP32;
           e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
         }
       } else {
         e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
       }
+      // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
+      c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
       c->launches++;
+      c->prof_begin();
       if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
+      // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
+      c->prof_end(ONTC_KCLASS_ADAM,
+                  s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0, 0.0);
       c->launches++;
       c->last_seed = s.seed;
       c->last_noise = s.noise != 0;
+      c->last_step = s;
       c->batch_i = bi + 1;
     }
   }
@@ -940,6 +992,213 @@ int ontc_get_step_losses(ontc_context* c, double* out, int32_t n)
 
 int64_t ontc_kernel_launch_count(ontc_context* c) { return c->launches; }
 
+int ontc_profile_kernels(ontc_context* c, int32_t enable)
+{
+  if (!c->initialized) return ONTC_INVALID_STATE;
+  cudaStreamSynchronize(c->stream);
+  for (auto& r : c->prof) {
+    c->event_pool.push_back(r.a);
+    c->event_pool.push_back(r.b);
+  }
+  c->prof.clear();
+  c->profiling = enable != 0;
+  return ONTC_SUCCESS;
+}
+
+int ontc_kernel_times(ontc_context* c, ontc_kernel_time* out, int32_t max_classes)
+{
+  if (!c->initialized || !out) return 0;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return 0;
+  int n = std::min<int>(max_classes, ONTC_KCLASS_COUNT);
+  for (int i = 0; i < n; i++) out[i] = ontc_kernel_time{};
+  for (auto& r : c->prof) {
+    if (r.cls >= n) continue;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    out[r.cls].launches += 1;
+    out[r.cls].total_ms += ms;
+    out[r.cls].bytes += r.bytes;
+    out[r.cls].flops += r.flops;
+  }
+  return n;
+}
+
 const char* ontc_version(void) { return "ontc 0.1 sm_100a"; }
+
+}  // extern "C"
+
+// ---- introspection (include/ontc_debug.h) ------------------------------------------------
+
+extern "C" {
+
+int64_t ontc_debug_tensor(ontc_context* c, int32_t which, int32_t level, float* host, int64_t n, int32_t to_device)
+{
+  float* dev = nullptr;
+  size_t count = 0;
+  if (which >= ONTC_DBG_G0 && which <= ONTC_DBG_G1_GRAD) {
+    if (!c->manifest_loaded || level < 0 || level >= c->levels) return -1;
+    static const int map_g[8] = {0, 1, 0, 0, 1, 1, 0, 1};
+    static const int map_k[8] = {0, 0, 1, 2, 1, 2, 3, 3};
+    const int g = map_g[which], k = map_k[which];
+    dev = c->lat[g][k][level].p;
+    count = c->level_elems(g, level);
+  } else if (which == ONTC_DBG_W || which == ONTC_DBG_W_M || which == ONTC_DBG_W_V) {
+    if (!c->initialized) return -1;
+    dev = which == ONTC_DBG_W ? c->W.p : which == ONTC_DBG_W_M ? c->Wm.p : c->Wv.p;
+    count = (size_t)c->nW;
+  } else if (which == ONTC_DBG_W_GRAD) {
+    if (to_device || c->last_dW.empty()) return -1;
+    if (n <= 0) return (int64_t)c->last_dW.size();
+    if ((size_t)n > c->last_dW.size()) return -1;
+    memcpy(host, c->last_dW.data(), n * sizeof(float));
+    return n;
+  } else {
+    return -1;
+  }
+  if (n <= 0) return (int64_t)count;
+  if ((size_t)n > count || !dev) return -1;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!e)
+    e = to_device ? cudaMemcpy(dev, host, n * sizeof(float), cudaMemcpyHostToDevice)
+                  : cudaMemcpy(host, dev, n * sizeof(float), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? n : -1;
+}
+
+int ontc_debug_last_step(ontc_context* c, ontc_debug_step* o)
+{
+  memset(o, 0, sizeof(*o));
+  const StepRec& s = c->last_step;
+  o->lod = s.lod;
+  o->n_grids = s.n_grids;
+  for (int i = 0; i < kMaxGrids; i++) {
+    o->ox[i] = s.ox[i];
+    o->oy[i] = s.oy[i];
+  }
+  o->noise = s.noise;
+  o->seed = s.seed;
+  o->step = s.step;
+  o->level = s.level;
+  o->lr_grid = s.lr_grid;
+  o->lr_dec = s.lr_dec;
+  o->b1 = s.b1;
+  o->b2 = s.b2;
+  o->gb1 = s.gb1;
+  o->gb2 = s.gb2;
+  o->grid_update = s.grid_update;
+  return ONTC_SUCCESS;
+}
+
+int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
+{
+  if (!c->manifest_loaded || d->lod < 0 || d->lod >= c->mips || d->n_grids < 1 || d->n_grids > kMaxGrids)
+    return ONTC_INVALID_STATE;
+  StepRec s = {};
+  s.lod = d->lod;
+  s.level = c->feature_level_for_lod(d->lod);
+  d->level = s.level;
+  s.mip_dim = c->mip_dim[d->lod];
+  s.tile_dim = std::min(s.mip_dim, 256);
+  s.n_grids = d->n_grids;
+  s.texels = s.n_grids * s.tile_dim * s.tile_dim;
+  s.noise = d->noise ? 1 : 0;
+  s.grid_update = 1;
+  s.seed = d->seed;
+  s.norm_lod = d->lod / static_cast<float>(c->mips - 1);
+  s.step = d->step;
+  for (int i = 0; i < kMaxGrids; i++) {
+    s.ox[i] = ((d->ox[i] % s.mip_dim) + s.mip_dim) % s.mip_dim;
+    s.oy[i] = ((d->oy[i] % s.mip_dim) + s.mip_dim) % s.mip_dim;
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  for (int g = 0; g < 2 && !e; g++)
+    e = cudaMemsetAsync(c->lat[g][3][s.level].p, 0, c->level_elems(g, s.level) * sizeof(float), c->stream);
+  if (!e) e = cudaMemcpyAsync(c->aux_steps.p, &s, sizeof(s), cudaMemcpyHostToDevice, c->stream);
+  const int units = (s.texels + kTile - 1) / kTile;
+  int grid = std::min(units, c->sms);
+  const Model M = c->model();
+  TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
+  if (!e) {
+    if (c->precision == ONTC_PRECISION_BF16) {
+      grid = std::min(units, tc_max_grid());
+      e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->stream);
+      if (e == cudaErrorNotSupported) {
+        cudaGetLastError();
+        grid = std::min(units, c->sms);
+        e = launch_simt_units(kTrain, M, c->aux_steps.p, 0, grid, to, c->stream);
+      }
+    } else {
+      e = launch_simt_units(kTrain, M, c->aux_steps.p, 0, grid, to, c->stream);
+    }
+    c->launches++;
+  }
+  std::vector<float> part((size_t)grid * c->nW);
+  std::vector<double> lp(grid);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (!e) e = cudaMemcpy(part.data(), c->dWpart.p, part.size() * sizeof(float), cudaMemcpyDeviceToHost);
+  if (!e) e = cudaMemcpy(lp.data(), c->loss_part.p, lp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e) return ONTC_CUDA_FAILURE;
+  c->last_dW.assign(c->nW, 0.0f);
+  for (int w = 0; w < c->nW; w++) {
+    double acc = 0.0;
+    for (int i = 0; i < grid; i++) acc += part[(size_t)i * c->nW + w];
+    c->last_dW[w] = (float)acc;
+  }
+  double l = 0.0;
+  for (double v : lp) l += v;
+  if (loss) *loss = l / ((double)c->C * s.texels);
+  return ONTC_SUCCESS;
+}
+
+int ontc_debug_quantize_pack(const float* host_in, int64_t n, int32_t bits, uint32_t* host_out)
+{
+  if (bits <= 0 || bits > 16 || (n * bits) % 32 != 0) return ONTC_INVALID_STATE;
+  DBuf<float> in;
+  DBuf<uint32_t> out;
+  const size_t words = (size_t)(n * bits / 32);
+  if (in.alloc(n) || out.alloc(words)) return ONTC_ALLOCATION_FAILURE;
+  cudaError_t e = cudaMemcpy(in.p, host_in, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (!e) e = launch_quantize_pack(in.p, n, bits, out.p, 0);
+  if (!e) e = cudaMemcpy(host_out, out.p, words * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int ontc_debug_lanczos_down(const uint8_t* src, int32_t dim, int32_t ch, uint8_t* dst)
+{
+  DBuf<uint8_t> s, d;
+  DBuf<float> tmp;
+  const size_t n = (size_t)dim * dim * ch;
+  if (s.alloc(n) || d.alloc(n / 4) || tmp.alloc(n / 2)) return ONTC_ALLOCATION_FAILURE;
+  cudaError_t e = cudaMemcpy(s.p, src, n, cudaMemcpyHostToDevice);
+  if (!e) e = launch_lanczos_down(s.p, dim, ch, tmp.p, d.p, 0);
+  if (!e) e = cudaMemcpy(dst, d.p, n / 4, cudaMemcpyDeviceToHost);
+  return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int ontc_debug_lanczos_weights(float* out12) { return lanczos_weights(out12) ? ONTC_CUDA_FAILURE : ONTC_SUCCESS; }
+
+int ontc_debug_package(ontc_context* c, int32_t mip, uint8_t* out)
+{
+  if (!c->manifest_loaded || mip < 0 || mip >= c->mips) return ONTC_INVALID_STATE;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!e) e = cudaMemcpy(out, c->package[mip].p, c->package[mip].n, cudaMemcpyDeviceToHost);
+  return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int ontc_debug_shape(ontc_context* c, int32_t* o)
+{
+  o[0] = c->F;
+  o[1] = c->Fp;
+  o[2] = c->C;
+  o[3] = c->mips;
+  o[4] = c->levels;
+  o[5] = c->nW;
+  for (int i = 0; i < 6; i++) o[6 + i] = i < c->levels ? c->g0_dim[i] : 0;
+  for (int i = 0; i < 6; i++) o[12 + i] = i < c->levels ? c->g1_dim[i] : 0;
+  for (int i = 0; i < 12; i++) o[18 + i] = i < c->mips ? c->mip_dim[i] : 0;
+  o[30] = c->batch_i;
+  o[31] = c->lock_i;
+  o[32] = c->batch_count;
+  return ONTC_SUCCESS;
+}
 
 }  // extern "C"

@@ -167,6 +167,9 @@ static float* tensor_ptr(Context* c, int which, int level, size_t* n)
     case 17: *n = c->vW0_.NumElems(); return c->vW0_.DevicePtr();
     case 18: *n = c->g0_noise_.NumElems(); return c->g0_noise_.DevicePtr();
     case 19: *n = c->g1_noise_.NumElems(); return c->g1_noise_.DevicePtr();
+    case 20: *n = c->x_.NumElems(); return c->x_.DevicePtr();      // features [F][max_batch]
+    case 21: *n = c->dLdx_.NumElems(); return c->dLdx_.DevicePtr();  // feature gradient [F][max_batch]
+    case 22: *n = c->Woutx_.NumElems(); return c->Woutx_.DevicePtr();  // predictions [16][max_batch]
     default: *n = 0; return nullptr;
   }
 }
