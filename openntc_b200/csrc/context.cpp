@@ -311,6 +311,15 @@ void unload(ontc_context* c)
   c->manifest_loaded = false;
 }
 
+// The tensor-core kernel reports a bounded-wait timeout through this word instead of
+// spinning; the context treats it as a CUDA failure.
+bool tc_failed(ontc_context* c)
+{
+  int flag = 0;
+  if (cudaMemcpy(&flag, c->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return true;
+  return flag != 0;
+}
+
 ontc_train_progress make_progress(int32_t phase, int32_t result, const ontc_context* c)
 {
   ontc_train_progress p = {};
@@ -855,6 +864,7 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
     }
   }
   if (!e) e = cudaStreamSynchronize(c->stream);
+  if (!e && tc_failed(c)) e = cudaErrorLaunchTimeout;
   if (e != cudaSuccess) {
     c->last_error = ONTC_CUDA_FAILURE;
     *out = make_progress(ONTC_TRAIN_ERROR, ONTC_CUDA_FAILURE, c);
@@ -1134,6 +1144,7 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
   std::vector<float> part((size_t)grid * c->nW);
   std::vector<double> lp(grid);
   if (!e) e = cudaStreamSynchronize(c->stream);
+  if (!e && tc_failed(c)) e = cudaErrorLaunchTimeout;
   if (!e) e = cudaMemcpy(part.data(), c->dWpart.p, part.size() * sizeof(float), cudaMemcpyDeviceToHost);
   if (!e) e = cudaMemcpy(lp.data(), c->loss_part.p, lp.size() * sizeof(double), cudaMemcpyDeviceToHost);
   if (e) return ONTC_CUDA_FAILURE;

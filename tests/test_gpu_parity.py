@@ -77,7 +77,8 @@ def test_lanczos_weights_close_to_libm(lib, oracle):
     wd = _device_weights(lib)
     wh = oracle.lanczos_weights()
     ulp = np.abs(wd.view(np.int32).astype(np.int64) - wh.view(np.int32).astype(np.int64))
-    assert ulp.max() <= 2, (wd, wh)
+    # CUDA sinf (<= 2 ulp) vs glibc sinf (<= 1 ulp); the reductions themselves are checked bit-exact
+    assert ulp.max() <= 4, (wd, wh)
 
 
 def _images(rng):
@@ -188,7 +189,8 @@ def test_step0_features_match_upstream(step0, oracle):
     F, mip = sh["F"], sh["mip_dim"][s.lod]
     T = min(mip, 256)
     B = step0["grids"] * T * T
-    X = ref.tensor(20, n=F * 8 * 65536).reshape(F, -1)[:, :B]
+    # upstream packs x_ as [F][B] with stride B (ntc_kernel.cu:128)
+    X = ref.tensor(20, n=F * B).reshape(F, B)
     m, level = H.oracle_model(oracle, ctx, step0["profile"], s.lod)
     ost = oracle.step(T, [(s.ox[i], s.oy[i]) for i in range(s.n_grids)], 0, 0, s.lod / (sh["mips"] - 1))
     rng = np.random.default_rng(0)
