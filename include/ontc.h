@@ -155,8 +155,16 @@ typedef struct ontc_train_options {
   int32_t has_lock_step;  /* !=0: use lock_step as the latent lock/snap step */
   int32_t lock_step;
   int32_t precision;      /* ONTC_PRECISION_* */
-  int32_t reserved[4];
+  int32_t noise_mode;     /* ONTC_NOISE_* */
+  int32_t reserved[3];
 } ontc_train_options;
+
+/* Quantisation-noise surrogate used before the latent lock.
+ *   COUNTER (default): U(-delta/2, delta/2) from a counter-based hash of (step, element),
+ *                      generated only at the latents a step touches; nothing stored.
+ *   UPSTREAM:          upstream's cuRAND XORWOW stream and level-wide noise buffers
+ *                      (ntc_kernel.cu:412-446), for trajectory parity with upstream. */
+enum { ONTC_NOISE_COUNTER = 0, ONTC_NOISE_UPSTREAM = 1 };
 
 typedef struct ontc_context ontc_context;
 typedef struct ontc_file ontc_file;

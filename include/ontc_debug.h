@@ -25,6 +25,8 @@ enum {
   ONTC_DBG_G1_V = 5,
   ONTC_DBG_G0_GRAD = 6, /* latent gradient buffers (zero between steps) */
   ONTC_DBG_G1_GRAD = 7,
+  ONTC_DBG_NOISE0 = 8,  /* upstream-mode noise buffers (level-0 sized; level argument ignored) */
+  ONTC_DBG_NOISE1 = 9,
   ONTC_DBG_W = 10,      /* decoder, fp32: W0 [64][F] | W1 [64][64] | Wout [16][64] */
   ONTC_DBG_W_M = 11,
   ONTC_DBG_W_V = 12,

@@ -70,6 +70,11 @@ class Precision(enum.IntEnum):
     FP32 = 1
 
 
+class NoiseMode(enum.IntEnum):
+    COUNTER = 0   # counter-based surrogate, generated at the touched latents only
+    UPSTREAM = 1  # upstream's cuRAND stream and level-wide buffers (trajectory parity)
+
+
 def load() -> C.CDLL:
     """Loads (once) and binds the in-tree libontc.so.  Raises if it was not built."""
     global _lib
@@ -112,13 +117,15 @@ class Context:
         self._lib.ontc_unload_manifest(self._h)
 
     def begin_training(self, quality: int, grids_per_batch: int = 1, steps: int | None = None,
-                       lock_step: int | None = None, precision: int = Precision.BF16):
+                       lock_step: int | None = None, precision: int = Precision.BF16,
+                       noise_mode: int = NoiseMode.COUNTER):
         self._lib.ontc_begin_training(self._h, int(quality), int(grids_per_batch))
         o = TrainOptions()
         o.steps_override = steps or 0
         o.has_lock_step = 1 if lock_step is not None else 0
         o.lock_step = lock_step or 0
         o.precision = int(precision)
+        o.noise_mode = int(noise_mode)
         r = self._lib.ontc_set_train_options(self._h, C.byref(o))
         if r != 0:
             raise RuntimeError(f"ontc_set_train_options: {Result(r).name}")

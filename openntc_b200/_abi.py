@@ -77,7 +77,10 @@ class TextureData(C.Structure):
 
 class TrainOptions(C.Structure):
     _fields_ = [("steps_override", C.c_int32), ("has_lock_step", C.c_int32), ("lock_step", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("precision", C.c_int32), ("noise_mode", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+NOISE_COUNTER, NOISE_UPSTREAM = 0, 1
 
 
 class KernelTime(C.Structure):
@@ -94,7 +97,7 @@ class DebugStep(C.Structure):
                 ("gb1", C.c_float), ("gb2", C.c_float), ("grid_update", C.c_int32), ("pad", C.c_int32)]
 
 
-DBG_G0, DBG_G1, DBG_G0_M, DBG_G0_V, DBG_G1_M, DBG_G1_V, DBG_G0_GRAD, DBG_G1_GRAD = range(8)
+DBG_G0, DBG_G1, DBG_G0_M, DBG_G0_V, DBG_G1_M, DBG_G1_V, DBG_G0_GRAD, DBG_G1_GRAD, DBG_NOISE0, DBG_NOISE1 = range(10)
 DBG_W, DBG_W_M, DBG_W_V, DBG_W_GRAD = 10, 11, 12, 13
 
 # name -> (restype, argtypes); every symbol include/ontc.h and include/ontc_debug.h declare.

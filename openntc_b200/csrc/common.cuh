@@ -65,6 +65,9 @@ struct Model {
   float* Wm;
   float* Wv;
   int32_t nW;  // 64*F + 64*64 + 16*64
+  // upstream-compatible noise buffers (StepRec::noise == 2), indexed like the level's latents
+  const float* noise0;
+  const float* noise1;
 };
 
 ONTC_HD int w0_off() { return 0; }
@@ -121,6 +124,17 @@ ONTC_HD float noise_value(uint32_t seed, uint32_t which, uint32_t e, float delta
   const float u = ((float)(noise_bits(seed, which, e) >> 8) + 0.5f) * (1.0f / 16777216.0f);
   return u * delta - 0.5f * delta;
 }
+
+// Noise added to latent element e of pyramid `which` in step s: none (noise == 0), the
+// counter-based surrogate (noise == 1), or upstream's cuRAND buffers (noise == 2).
+#if defined(__CUDACC__)
+__device__ __forceinline__ float latent_noise(const Model& M, const StepRec& s, uint32_t which, uint32_t e)
+{
+  if (s.noise == 1) return noise_value(s.seed, which, e, which == 0 ? M.g0.delta : M.g1.delta);
+  if (s.noise == 2) return which == 0 ? M.noise0[e] : M.noise1[e];
+  return 0.0f;
+}
+#endif
 
 // hardgelu and its derivative (ntc_kernel.cu:50-62)
 ONTC_HD float hardgelu(float x)

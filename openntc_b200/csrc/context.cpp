@@ -145,6 +145,7 @@ struct ontc_context {
   int32_t batch_count = 0, batch_i = 0, lock_i = 0, grids = 1;
   int32_t grid_batch_i[ONTC_MAX_LEVELS] = {};
   int32_t precision = ONTC_PRECISION_BF16;
+  int32_t noise_mode = ONTC_NOISE_COUNTER;
   uint32_t last_seed = 0;
   bool last_noise = false;
   std::mt19937 gen{123};
@@ -161,6 +162,9 @@ struct ontc_context {
   DBuf<uint8_t> package[ONTC_MAX_MIPS];
   DBuf<uint32_t> packbuf;
   DBuf<int> tc_error;
+  DBuf<uint8_t> noise_states;   // upstream-mode cuRAND states (initialised once per context)
+  DBuf<float> noise_buf[2];     // upstream-mode level noise buffers, level-0 sized
+  static constexpr int kNoiseStates = 1 << 20;  // libopenntc.cpp:377 rand_dim_
   StepRec* h_steps = nullptr;  // pinned staging
   size_t h_steps_cap = 0;
 
@@ -246,6 +250,8 @@ struct ontc_context {
     M.Wm = Wm.p;
     M.Wv = Wv.p;
     M.nW = nW;
+    M.noise0 = noise_buf[0].p;
+    M.noise1 = noise_buf[1].p;
     return M;
   }
 
@@ -287,7 +293,8 @@ StepRec full_mip_rec(const ontc_context* c, int mip)
   s.tile_dim = c->mip_dim[mip];
   s.n_grids = 1;
   s.texels = c->mip_dim[mip] * c->mip_dim[mip];
-  s.noise = c->last_noise ? 1 : 0;
+  // upstream's Eval/Calibrate add whatever its noise buffers hold (zero after the lock)
+  s.noise = c->noise_mode == ONTC_NOISE_UPSTREAM ? 2 : (c->last_noise ? 1 : 0);
   s.seed = c->last_seed;
   s.norm_lod = mip / static_cast<float>(c->mips - 1);
   s.step = 0;
@@ -303,6 +310,8 @@ void unload(ontc_context* c)
   for (int i = 0; i < ONTC_MAX_MIPS; i++) c->package[i].release();
   c->packbuf.release();
   c->losses.release();
+  c->noise_buf[0].release();
+  c->noise_buf[1].release();
   c->g0_host_packed.clear();
   c->g1_host_packed.clear();
   for (int i = 0; i < ONTC_MAX_LEVELS; i++) c->g0_host[i] = c->g1_host[i] = nullptr;
@@ -747,6 +756,22 @@ int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
     }
   }
   if (o->has_lock_step) c->lock_i = std::max(0, o->lock_step);
+  if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
+  c->noise_mode = o->noise_mode;
+  if (c->noise_mode == ONTC_NOISE_UPSTREAM) {
+    if (!c->manifest_loaded) return ONTC_INVALID_STATE;
+    if (!c->noise_states.p) {
+      if (c->noise_states.alloc(noise_state_bytes(ontc_context::kNoiseStates))) return ONTC_ALLOCATION_FAILURE;
+      if (launch_noise_init(c->noise_states.p, ontc_context::kNoiseStates, c->stream)) return ONTC_CUDA_FAILURE;
+      c->launches++;
+    }
+    for (int g = 0; g < 2; g++) {
+      if (!c->noise_buf[g].p) {
+        if (c->noise_buf[g].alloc(c->level_elems(g, 0))) return ONTC_ALLOCATION_FAILURE;
+        if (cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream)) return ONTC_CUDA_FAILURE;
+      }
+    }
+  }
   return ONTC_SUCCESS;
 }
 
@@ -805,7 +830,7 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       s.tile_dim = std::min(c->mip_dim[lod], 256);
       s.n_grids = c->grids;
       s.texels = c->grids * s.tile_dim * s.tile_dim;
-      s.noise = bi < c->lock_i ? 1 : 0;
+      s.noise = bi < c->lock_i ? (c->noise_mode == ONTC_NOISE_UPSTREAM ? 2 : 1) : 0;
       s.grid_update = bi < c->lock_i ? 1 : 0;
       s.seed = step_seed((uint32_t)bi);
       s.norm_lod = lod / static_cast<float>(c->mips - 1);
@@ -822,6 +847,13 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
     for (int k = 0; k < cnt && e == cudaSuccess; k++) {
       const int bi = first + k;
       const StepRec& s = c->h_steps[k];
+      if (c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
+        // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
+        for (int g = 0; g < 2 && e == cudaSuccess; g++)
+          e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
+                                g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
+        c->launches += 2;
+      }
       if (bi == c->lock_i) {
         // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
         for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
@@ -829,6 +861,8 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
           if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
           c->launches += 2;
         }
+        for (int g = 0; g < 2 && e == cudaSuccess; g++)
+          if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
       }
       const int units = (s.texels + kTile - 1) / kTile;
       TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
@@ -1052,6 +1086,11 @@ int64_t ontc_debug_tensor(ontc_context* c, int32_t which, int32_t level, float* 
     const int g = map_g[which], k = map_k[which];
     dev = c->lat[g][k][level].p;
     count = c->level_elems(g, level);
+  } else if (which == ONTC_DBG_NOISE0 || which == ONTC_DBG_NOISE1) {
+    const int g = which - ONTC_DBG_NOISE0;
+    dev = c->noise_buf[g].p;
+    count = c->noise_buf[g].n;
+    if (!dev) return -1;
   } else if (which == ONTC_DBG_W || which == ONTC_DBG_W_M || which == ONTC_DBG_W_V) {
     if (!c->initialized) return -1;
     dev = which == ONTC_DBG_W ? c->W.p : which == ONTC_DBG_W_M ? c->Wm.p : c->Wv.p;

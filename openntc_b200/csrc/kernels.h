@@ -40,6 +40,11 @@ cudaError_t launch_fill(float* p, long long n, float v, cudaStream_t stream);
 // out = sum over the first n doubles (single CTA, deterministic order)
 cudaError_t launch_sum_doubles(const double* in, int n, double* out, cudaStream_t stream);
 
+// ---- upstream-compatible noise (parity mode)
+size_t noise_state_bytes(int n_states);
+cudaError_t launch_noise_init(void* states, int n_states, cudaStream_t stream);
+cudaError_t launch_noise_fill(void* states, int n_states, long long n, float delta, float* out, cudaStream_t stream);
+
 // ---- mip chain (LoadManifest)
 // picks `cmap_count` channels (cmap[i] in 0..3) out of an RGBA8 image into [dim][dim][count]
 cudaError_t launch_prepare(const uint8_t* rgba, int dim, const int* cmap, int count, uint8_t* out, cudaStream_t stream);

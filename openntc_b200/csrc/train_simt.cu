@@ -73,7 +73,7 @@ __device__ void gather_unit(const Model& M, const StepRec& s, const Smem& sm, bo
       const int base = G.c0[k] * C0;
       for (int c = 0; c < C0; c++) {
         float v = p0[base + c];
-        if (with_noise) v = v + noise_value(s.seed, 0u, (uint32_t)(base + c), M.g0.delta);
+        if (with_noise) v = v + latent_noise(M, s, 0u, (uint32_t)(base + c));
         sm.X[(k * C0 + c) * S + t] = v;
       }
     }
@@ -85,7 +85,7 @@ __device__ void gather_unit(const Model& M, const StepRec& s, const Smem& sm, bo
       for (int k = 0; k < 4; k++) {
         const int e = G.c1[k] * C1 + c;
         float v = p1[e];
-        if (with_noise) v = v + noise_value(s.seed, 1u, (uint32_t)e, M.g1.delta);
+        if (with_noise) v = v + latent_noise(M, s, 1u, (uint32_t)e);
         acc = __fmaf_rn(G.w1[k], v, acc);
       }
       sm.X[(4 * C0 + c) * S + t] = acc;

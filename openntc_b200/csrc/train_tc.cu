@@ -122,7 +122,7 @@ __device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, con
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           float val = v[i];
-          if (s.noise) val = val + noise_value(s.seed, 0u, (uint32_t)(base + c + i), M.g0.delta);
+          if (s.noise) val = val + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
           buf[f & 7] = val;
           f++;
         }
@@ -139,8 +139,8 @@ __device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, con
         const float2 q = *reinterpret_cast<const float2*>(p1 + base + c);
         float a = q.x, b = q.y;
         if (s.noise) {
-          a = a + noise_value(s.seed, 1u, (uint32_t)(base + c), M.g1.delta);
-          b = b + noise_value(s.seed, 1u, (uint32_t)(base + c + 1), M.g1.delta);
+          a = a + latent_noise(M, s, 1u, (uint32_t)(base + c));
+          b = b + latent_noise(M, s, 1u, (uint32_t)(base + c + 1));
         }
         acc[c] = __fmaf_rn(G.w1[k], a, acc[c]);
         acc[c + 1] = __fmaf_rn(G.w1[k], b, acc[c + 1]);

@@ -125,16 +125,49 @@ def test_midtraining_eval_includes_live_noise(trained, oracle):
     assert trained["mid"].psnr > 10.0 and trained["mid_step"].noise == 1
 
 
-def test_psnr_matches_upstream_at_equal_steps(materials):
+@pytest.fixture(scope="module")
+def upstream_cls():
     from oracle.bindings import REF_SO, RefContext
     if not REF_SO.exists():
         pytest.skip("upstream build missing")
+    return RefContext
+
+
+def test_upstream_noise_buffers_match(materials, upstream_cls):
+    """Parity mode reproduces upstream's cuRAND noise buffers bit for bit, step after step."""
+    profile, grids = ont.Profile.Bpp_0_5, 1
+    manifest = materials(1024, 0, 9)
+    ctx = H.new_context(profile, manifest, min_dim=1024, grids=grids, steps=1000, noise_mode=ont.NoiseMode.UPSTREAM)
+    ref = upstream_cls(profile)
+    try:
+        assert ref.load_manifest(manifest) == 0
+        ref.begin_training(0, grids, 1000, -1)
+        sh = H.shape(ctx)
+        for step in range(3):
+            ctx.train(1)
+            ref.train(1)
+            s = H.last_step(ctx)
+            for which, rwhich in ((_abi.DBG_NOISE0, 18), (_abi.DBG_NOISE1, 19)):
+                n = (sh["g0"][s.level] ** 2) * H.PROFILE_SHAPES[profile][2] if which == _abi.DBG_NOISE0 else \
+                    (sh["g1"][s.level] ** 2) * H.PROFILE_SHAPES[profile][3]
+                mine = H.tensor(ctx, which, 0)[:n]
+                theirs = ref.tensor(rwhich, 0)[:n]
+                assert np.array_equal(mine, theirs), (step, which, np.abs(mine - theirs).max())
+    finally:
+        ref.close()
+
+
+@pytest.mark.parametrize("precision", [ont.Precision.FP32, ont.Precision.BF16])
+def test_psnr_matches_upstream_at_equal_steps(materials, upstream_cls, precision):
+    """Same seed, draws, init and (parity-mode) noise: final PSNR within 0.1 dB of upstream."""
     profile, steps, grids = ont.Profile.Bpp_0_5, 1000, 1
     manifest = materials(1024, 0, 9)
-    ctx = H.new_context(profile, manifest, min_dim=1024, grids=grids, steps=steps)
-    ctx.train_until_complete()
+    ctx = H.new_context(profile, manifest, min_dim=1024, grids=grids, steps=steps, precision=precision,
+                        noise_mode=ont.NoiseMode.UPSTREAM)
+    p = ctx.train_until_complete()
+    assert p.phase == ont.TrainPhase.TrainComplete
     mine = ctx.eval().psnr
-    ref = RefContext(profile)
+    ref = upstream_cls(profile)
     try:
         assert ref.load_manifest(manifest) == 0
         ref.begin_training(0, grids, steps, -1)
@@ -142,5 +175,5 @@ def test_psnr_matches_upstream_at_equal_steps(materials):
         _, theirs = ref.eval()
     finally:
         ref.close()
-    print(f"PSNR after {steps} steps: libontc fp32 {mine:.3f} dB, upstream {theirs:.3f} dB")
+    print(f"PSNR after {steps} steps: libontc {precision.name} {mine:.3f} dB, upstream {theirs:.3f} dB")
     assert abs(mine - theirs) < 0.1
