@@ -77,27 +77,50 @@ ONTC_HD int n_weights(int F) { return kHidden * F + kHidden * kHidden + kOutPad 
 
 ONTC_HD int clampi(int x, int a, int b) { return x > b ? b : (x < a ? a : x); }
 
+// log2 of a power of two, and its exact reciprocal: every texture, grid and tile dimension
+// here is a power of two, so x / n == x * rcp_pow2(n) bit for bit and the divisions and
+// modulos become shifts and masks.
+ONTC_HD int log2_pow2(int n)
+{
+#if defined(__CUDA_ARCH__)
+  return __ffs(n) - 1;
+#else
+  return __builtin_ctz((unsigned)n);
+#endif
+}
+ONTC_HD float rcp_pow2(int n)
+{
+  const uint32_t bits = (uint32_t)(127 - log2_pow2(n)) << 23;
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(bits);
+#else
+  float f;
+  __builtin_memcpy(&f, &bits, 4);
+  return f;
+#endif
+}
+
 // Texel b of a step's batch -> mip-space (x, y).  Tiles are tile_dim x tile_dim blocks at
 // the drawn origins, wrapping mod mip_dim (ntc_kernel.cu:94-99); inside a tile, 128-texel
 // work units are 16x8 texel blocks (tile_dim >= 16) so one unit's latent footprint is
 // compact, or plain rows for the 4x4 and 8x8 tiles of the smallest mips.
 ONTC_HD void texel_xy(const StepRec& s, int b, int& x, int& y)
 {
-  const int T = s.tile_dim;
-  const int TT = T * T;
-  const int gi = b / TT;
-  const int r = b - gi * TT;
+  const int lt = log2_pow2(s.tile_dim);  // tile_dim and mip_dim are powers of two
+  const int gi = b >> (2 * lt);
+  const int r = b & ((1 << (2 * lt)) - 1);
   int lx, ly;
-  if (T >= 16) {
-    const int blk = r >> 7, i = r & 127, bpr = T >> 4;
-    lx = (blk % bpr) * 16 + (i & 15);
-    ly = (blk / bpr) * 8 + (i >> 4);
+  if (lt >= 4) {
+    const int blk = r >> 7, i = r & 127, lb = lt - 4;  // 2^lb 16-wide blocks per block row
+    lx = ((blk & ((1 << lb) - 1)) << 4) + (i & 15);
+    ly = ((blk >> lb) << 3) + (i >> 4);
   } else {
-    lx = r % T;
-    ly = r / T;
+    lx = r & ((1 << lt) - 1);
+    ly = r >> lt;
   }
-  x = (lx + s.ox[gi]) % s.mip_dim;
-  y = (ly + s.oy[gi]) % s.mip_dim;
+  const int mask = s.mip_dim - 1;
+  x = (lx + s.ox[gi]) & mask;
+  y = (ly + s.oy[gi]) & mask;
 }
 
 // Quantisation-noise surrogate U(-delta/2, delta/2) for latent element e of pyramid
@@ -160,8 +183,9 @@ struct Gather {
 
 ONTC_HD void gather_geometry(int x, int y, int mip_dim, int g0_dim, int g1_dim, Gather& G)
 {
-  const float u = ((float)x + 0.5f) / (float)mip_dim;
-  const float v = ((float)y + 0.5f) / (float)mip_dim;
+  const float rm = rcp_pow2(mip_dim);  // exact: (x + 0.5) / mip_dim
+  const float u = ((float)x + 0.5f) * rm;
+  const float v = ((float)y + 0.5f) * rm;
   // u * dim is exact (power-of-two dims), so fused and unfused forms agree here
   const float g0x = u * (float)g0_dim - 0.5f;
   const float g0y = v * (float)g0_dim - 0.5f;
@@ -190,7 +214,7 @@ ONTC_HD float pos_enc(int x, int y, int idx)
   const float P = (float)(8 >> p);
   const float c = (float)(a == 0 ? x : y);
   const float phase = h == 0 ? 0.0f : 0.25f * P;
-  const float t = (c + 0.5f + phase) / P;
+  const float t = (c + 0.5f + phase) * (0.125f * (float)(1 << p));  // exact: / P
   const float s = t - floorf(t);
   return 1.0f - 4.0f * fabsf(s - 0.5f);
 }

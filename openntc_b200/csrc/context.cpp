@@ -870,7 +870,7 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       int cls = ONTC_KCLASS_UNITS_FP32;
       c->prof_begin();
       if (c->precision == ONTC_PRECISION_BF16) {
-        grid = std::min(units, tc_max_grid());
+        grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
         cls = ONTC_KCLASS_UNITS_BF16;
         e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
         if (e == cudaErrorNotSupported) {
@@ -1168,7 +1168,7 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
   TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
   if (!e) {
     if (c->precision == ONTC_PRECISION_BF16) {
-      grid = std::min(units, tc_max_grid());
+      grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
       e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->stream);
       if (e == cudaErrorNotSupported) {
         cudaGetLastError();

@@ -1,26 +1,29 @@
 // BF16 tensor-core tile kernel for one training step (sm_100a, tcgen05 + TMEM).
 //
-// Each CTA owns 128-texel work units in turn (persistent grid).  Per unit, the whole
-// per-texel pipeline of upstream's step runs on chip:
+// A CTA (one per SM, persistent) runs two independent 4-warp groups.  Each group owns one
+// 128-texel work unit at a time (thread = texel row = TMEM lane) and takes it through the
+// whole per-texel pipeline of upstream's step:
 //
-//   gather (ntc_kernel.cu:75-177)             -> sX   [128 x Kp]  bf16, shared memory
-//   H0 = X  W0^T          (M128 N64  K=Kp)    -> TMEM, epilogue: A0 = hg(H0) -> sA0
-//   H1 = A0 W1^T          (M128 N64  K=64)    -> TMEM, epilogue: A1 = hg(H1) -> sA1
-//   Y  = A1 Wout^T        (M128 N16  K=64)    -> TMEM, epilogue: dY = -2(t-y)/(C B) -> sdY
-//   dA1 = dY Wout         (M128 N64  K=16)    -> TMEM, epilogue: dH1 = dA1 hg'(H1) -> sdH1
-//   dA0 = dH1 W1          (M128 N64  K=64)    -> TMEM, epilogue: dH0 = dA0 hg'(H0) -> sdH0
+//   gather (ntc_kernel.cu:75-177)             -> X    [128 x Kp]  bf16, shared memory
+//   H0 = X  W0^T          (M128 N64  K=Kp)    -> TMEM, epilogue: A0 = hg(H0)
+//   H1 = A0 W1^T          (M128 N64  K=64)    -> TMEM, epilogue: A1 = hg(H1)
+//   Y  = A1 Wout^T        (M128 N16  K=64)    -> TMEM, epilogue: dY = -2(t-y)/(C B), loss
+//   dA1 = dY Wout         (M128 N64  K=16)    -> TMEM, epilogue: dH1 = dA1 hg'(H1)
+//   dA0 = dH1 W1          (M128 N64  K=64)    -> TMEM, epilogue: dH0 = dA0 hg'(H0)
 //   dX  = dH0 W0          (M128 N=Kp K=64)    -> TMEM, epilogue: scatter-add into the latent
 //                                                gradients (ntc_kernel.cu:280-341)
-// and the weight gradients accumulate in TMEM across all of the CTA's units:
+// while the weight gradients of both groups accumulate in shared TMEM accumulators:
 //   dWout^T += A1^T dY (M64 N16), dW1 += dH1^T A0 (M64 N64), dW0 += dH0^T X (M64 N=Kp),
-// K = 128 texels each, written once per CTA to its partial-sum slot.
+// K = 128 texels each, written once per CTA to its partial-sum slot (libopenntc.cpp:672-693).
 //
-// Every operand lives in shared memory in the no-swizzle canonical layout; an activation
-// tile [128 texels][n] serves as the K-major A operand of the next layer and, unchanged, as
-// the MN-major operand of the weight-gradient products.  Hidden pre-activations stay in
-// registers for the backward (no recompute pass, nothing stored to HBM).  One thread issues
-// the MMAs and commits them to an mbarrier; every wait is bounded and reports a timeout
-// through the error word instead of spinning forever.
+// The two groups synchronise only with themselves (named barriers, one mbarrier each), so
+// one group's epilogue math runs while the other's MMAs execute.  Operands sit in shared
+// memory in the no-swizzle canonical layout; a [128 texels][n] activation tile is the
+// K-major A operand of the next layer and, unchanged, the MN-major operand of the
+// weight-gradient products.  A0 and dH0 share a buffer, as do A1 and dH1 (each is dead
+// before its partner is written).  The latent footprint of a unit is staged once in shared
+// memory (noise added once per latent) and its gradient reduced there before one global add
+// per latent.  Every wait is bounded and reports a timeout through the error word.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -31,47 +34,48 @@ namespace ontc {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;      // 2 groups x 128
+constexpr int kGroupThreads = 128;
 constexpr uint32_t kTmemCols = 512;
-// TMEM column map
-constexpr uint32_t kColH = 0;      // H0 / H1 / dA1 / dA0   (64)
-constexpr uint32_t kColY = 64;     // Y                      (16)
-constexpr uint32_t kColDX = 128;   // dX                     (<= 96)
-constexpr uint32_t kColW0 = 256;   // dW0 accumulator, M=64  (<= 96)
-constexpr uint32_t kColW1 = 384;   // dW1 accumulator, M=64  (64)
-constexpr uint32_t kColWo = 448;   // dWout^T accumulator    (16)
+// TMEM column map: per group a 128-column window [128 g, 128 g + 128) holding
+//   H0/H1/dA1/dA0 at +0 (64), Y at +64 (16), and later dX at +0 (<= 96);
+// the shared weight-gradient accumulators (M=64 layout) follow.
+constexpr uint32_t kColW0 = 256;   // dW0     (<= 96 columns)
+constexpr uint32_t kColW1 = 352;   // dW1     (64)
+constexpr uint32_t kColWo = 416;   // dWout^T (16)
+constexpr int kFootFloats = 6144;  // per group, 24 KB
+constexpr int kMaxBoxW = 64;       // latent box limits of the owner-computes scatter
+constexpr int kMaxBoxH = 32;
 
-struct TcSmem {
-  uint8_t* X;    // [128][Kp]
-  uint8_t* A0;   // [128][64]
-  uint8_t* A1;   // [128][64]
-  uint8_t* dY;   // [128][16]
-  uint8_t* dH1;  // [128][64]
-  uint8_t* dH0;  // [128][64]
-  uint8_t* W0;   // [64][Kp]
-  uint8_t* W1;   // [64][64]
-  uint8_t* Wo;   // [16][64]
+template <int C0_, int C1_, int KP_>
+struct Shape {
+  static constexpr int C0 = C0_, C1 = C1_, Kp = KP_;
+  static constexpr int F = ((4 * C0 + C1 + 13 + 3) / 4) * 4;
+  static constexpr uint32_t SX = (Kp / 8) * 128;  // 8-row group stride of a [*][Kp] tile
 };
 
-__host__ __device__ inline size_t tc_smem_bytes(int Kp)
+constexpr uint32_t S64 = 8 * 128;  // 8-row group stride of a [*][64] tile
+constexpr uint32_t S16 = 2 * 128;  // ... of a [*][16] tile
+
+template <class SH>
+struct GroupSmem {
+  static constexpr size_t kX = 128 * SH::Kp * 2, kP = 128 * 64 * 2, kY = 128 * 16 * 2, kFoot = kFootFloats * 4;
+  static constexpr size_t kBytes = kX + 2 * kP + kY + kFoot;
+};
+
+template <class SH>
+constexpr size_t smem_bytes()
 {
-  return (size_t)128 * Kp * 2 + 4 * 128 * 64 * 2 + 128 * 16 * 2 + 64 * Kp * 2 + 64 * 64 * 2 + 16 * 64 * 2 + 1024;
+  return 2 * GroupSmem<SH>::kBytes + 64 * SH::Kp * 2 + 64 * 64 * 2 + 16 * 64 * 2 + 1024;
 }
 
-__device__ __forceinline__ TcSmem tc_carve(uint8_t* base, int Kp)
-{
-  TcSmem s;
-  s.X = base;
-  s.A0 = s.X + 128 * Kp * 2;
-  s.A1 = s.A0 + 128 * 64 * 2;
-  s.dY = s.A1 + 128 * 64 * 2;
-  s.dH1 = s.dY + 128 * 16 * 2;
-  s.dH0 = s.dH1 + 128 * 64 * 2;
-  s.W0 = s.dH0 + 128 * 64 * 2;
-  s.W1 = s.W0 + 64 * Kp * 2;
-  s.Wo = s.W1 + 64 * 64 * 2;
-  return s;
-}
+struct GroupPtrs {
+  uint8_t* X;    // [128][Kp]
+  uint8_t* P0;   // [128][64]  A0, later dH0
+  uint8_t* P1;   // [128][64]  A1, later dH1
+  uint8_t* dY;   // [128][16]
+  float* foot;   // [kFootFloats]
+};
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
 {
@@ -90,51 +94,214 @@ __device__ __forceinline__ void st_chunk(uint8_t* base, int r, int c0, int cols,
   *reinterpret_cast<uint4*>(base + ptx::cm_off16(r, c0, cols)) = q;
 }
 
-struct Unit {
-  int x, y;
-  bool valid;
+__device__ __forceinline__ void bar_group(int g) { asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory"); }
+
+// hardgelu and its derivative for the bf16 path: the division by 3 becomes a multiply by
+// the fp32 reciprocal (the operands are bf16-rounded anyway).
+__device__ __forceinline__ float hg_fast(float x)
+{
+  return x < -1.5f ? 0.0f : (x < 1.5f ? x * (x + 1.5f) * (1.0f / 3.0f) : x);
+}
+__device__ __forceinline__ float hg_grad_fast(float x)
+{
+  return x < -1.5f ? 0.0f : (x < 1.5f ? (2.0f * x + 1.5f) * (1.0f / 3.0f) : 1.0f);
+}
+
+// ---- latent footprint of a unit ---------------------------------------------------------
+struct Foot {
+  int x0, y0, w, h;
 };
 
-// Gathers one texel's features into row `row` of sX.  half 0 writes the 4*C0 g0 corner
-// features; half 1 the C1 bilinear g1 features, positional encodings, lod and zero pad.
-__device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, const Unit& u, int row, int half, int Kp,
-                                           uint8_t* sX)
+__device__ __forceinline__ void foot_span(int a, int b, int mip, int gd, int& lo, int& n)
+{
+  // corner cells of texels a..b: gather_geometry's arithmetic, clamped the same way
+  const float rm = rcp_pow2(mip);
+  const float ua = ((float)a + 0.5f) * rm, ub = ((float)b + 0.5f) * rm;
+  const int l = (int)floorf(ua * (float)gd - 0.5f), h = (int)floorf(ub * (float)gd - 0.5f) + 1;
+  lo = clampi(l, 0, gd - 1);
+  n = clampi(h, 0, gd - 1) - lo + 1;
+}
+
+// True when the unit is a 16x8 texel block that does not wrap and whose g0/g1 boxes fit.
+template <class SH>
+__device__ __forceinline__ bool unit_footprint(const Model& M, const StepRec& s, int unit, Foot& f0, Foot& f1)
+{
+  const int lt = log2_pow2(s.tile_dim);
+  if (lt < 4) return false;
+  const int b0 = unit * kTile, gi = b0 >> (2 * lt), r0 = b0 & ((1 << (2 * lt)) - 1);
+  const int blk = r0 >> 7, lb = lt - 4;
+  const int mask = s.mip_dim - 1;
+  const int xa = (((blk & ((1 << lb) - 1)) << 4) + s.ox[gi]) & mask;
+  const int ya = (((blk >> lb) << 3) + s.oy[gi]) & mask;
+  if (xa + 16 > s.mip_dim || ya + 8 > s.mip_dim) return false;
+  const int d0 = M.g0.dim[s.level], d1 = M.g1.dim[s.level];
+  foot_span(xa, xa + 15, s.mip_dim, d0, f0.x0, f0.w);
+  foot_span(ya, ya + 7, s.mip_dim, d0, f0.y0, f0.h);
+  foot_span(xa, xa + 15, s.mip_dim, d1, f1.x0, f1.w);
+  foot_span(ya, ya + 7, s.mip_dim, d1, f1.y0, f1.h);
+  return f0.w <= kMaxBoxW && f0.h <= kMaxBoxH && f1.w <= kMaxBoxW && f1.h <= kMaxBoxH &&
+         f0.w * f0.h * SH::C0 + f1.w * f1.h * SH::C1 <= kFootFloats;
+}
+
+// Which texel columns / rows of a unit touch each box column / row, per corner side: bit t
+// of lo[i] is set when texel t's lower corner cell is box cell i, of hi[i] for its upper one.
+// With these, the owner of a latent element sums exactly the texel-corner contributions
+// the per-texel scatter would have added (ntc_kernel.cu:317-340), without atomics.
+struct CornerMasks {
+  uint32_t xlo[2][kMaxBoxW], xhi[2][kMaxBoxW];  // [g0/g1][box column]
+  uint32_t ylo[2][kMaxBoxH], yhi[2][kMaxBoxH];
+  float fx[16], fy[8];                          // g1 bilinear fractions of the unit's columns / rows
+};
+
+__device__ __forceinline__ void build_masks(const StepRec& s, int d0, int d1, const Foot& f0, const Foot& f1,
+                                            int unit, CornerMasks& cm, int gt)
+{
+  // thread 0..15: texel column xa + gt; 16..23: texel row ya + gt - 16
+  const int lt = log2_pow2(s.tile_dim);
+  const int b0 = unit * kTile, gi = b0 >> (2 * lt), r0 = b0 & ((1 << (2 * lt)) - 1);
+  const int blk = r0 >> 7, lb = lt - 4;
+  const int mask = s.mip_dim - 1;
+  const float rm = rcp_pow2(s.mip_dim);
+  if (gt < 24) {
+    const bool col = gt < 16;
+    const int t = col ? gt : gt - 16;
+    const int p = col ? ((((blk & ((1 << lb) - 1)) << 4) + s.ox[gi]) & mask) + t
+                      : ((((blk >> lb) << 3) + s.oy[gi]) & mask) + t;
+    const float u = ((float)p + 0.5f) * rm;  // gather_geometry's arithmetic
+    for (int g = 0; g < 2; g++) {
+      const int gd = g == 0 ? d0 : d1;
+      const float q = u * (float)gd - 0.5f;
+      const float fq = floorf(q);
+      const int lo = clampi((int)fq, 0, gd - 1), hi = clampi((int)fq + 1, 0, gd - 1);
+      const Foot& f = g == 0 ? f0 : f1;
+      if (col) {
+        atomicOr(&cm.xlo[g][lo - f.x0], 1u << t);
+        atomicOr(&cm.xhi[g][hi - f.x0], 1u << t);
+        if (g == 1) cm.fx[t] = q - fq;
+      } else {
+        atomicOr(&cm.ylo[g][lo - f.y0], 1u << t);
+        atomicOr(&cm.yhi[g][hi - f.y0], 1u << t);
+        if (g == 1) cm.fy[t] = q - fq;
+      }
+    }
+  }
+}
+
+// Copies the unit's latent boxes (plus this step's noise) into shared memory.
+template <class SH>
+__device__ __forceinline__ void stage_footprint(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
+                                                float* foot, int gt)
 {
   const int lvl = s.level;
-  const int C0 = M.C0, C1 = M.C1;
-  if (!u.valid) {
+  {
+    constexpr int C0 = SH::C0;
+    const int d0 = M.g0.dim[lvl];
+    const int rowq = f0.w * (C0 / 4);
+    const float* p0 = M.g0.p[lvl];
+    for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
+      const int r = v / rowq, q = v - r * rowq;
+      const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
+      float4 val = *reinterpret_cast<const float4*>(p0 + e);
+      if (s.noise) {
+        val.x += latent_noise(M, s, 0u, (uint32_t)e);
+        val.y += latent_noise(M, s, 0u, (uint32_t)(e + 1));
+        val.z += latent_noise(M, s, 0u, (uint32_t)(e + 2));
+        val.w += latent_noise(M, s, 0u, (uint32_t)(e + 3));
+      }
+      *reinterpret_cast<float4*>(foot + r * f0.w * C0 + q * 4) = val;
+    }
+  }
+  {
+    constexpr int C1 = SH::C1;
+    const int d1 = M.g1.dim[lvl];
+    const int rowh = f1.w * (C1 / 2);
+    const float* p1 = M.g1.p[lvl];
+    float* foot1 = foot + f0.w * f0.h * SH::C0;
+    for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
+      const int r = v / rowh, q = v - r * rowh;
+      const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
+      float2 val = *reinterpret_cast<const float2*>(p1 + e);
+      if (s.noise) {
+        val.x += latent_noise(M, s, 1u, (uint32_t)e);
+        val.y += latent_noise(M, s, 1u, (uint32_t)(e + 1));
+      }
+      *reinterpret_cast<float2*>(foot1 + r * f1.w * C1 + q * 2) = val;
+    }
+  }
+}
+
+// Gathers one texel's feature row (draw_features arithmetic).  `staged` reads the latents
+// (noise already added) from the shared-memory boxes, otherwise from global memory.
+template <class SH>
+__device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, int x, int y, bool valid, int row,
+                                          bool staged, const Foot& f0, const Foot& f1, const float* foot, uint8_t* sX)
+{
+  constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
+  if (!valid) {
     const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int lo = half == 0 ? 0 : 4 * C0, hi = half == 0 ? 4 * C0 : Kp;
-    for (int c = lo; c < hi; c += 8) st_chunk(sX, row, c, Kp, z);
+#pragma unroll
+    for (int c = 0; c < Kp; c += 8) st_chunk(sX, row, c, Kp, z);
     return;
   }
+  const int lvl = s.level;
+  const int d0 = M.g0.dim[lvl], d1 = M.g1.dim[lvl];
+  const int l0 = log2_pow2(d0), l1 = log2_pow2(d1);
   Gather G;
-  gather_geometry(u.x, u.y, s.mip_dim, M.g0.dim[lvl], M.g1.dim[lvl], G);
+  gather_geometry(x, y, s.mip_dim, d0, d1, G);
   float buf[8];
-  if (half == 0) {
-    const float* p0 = M.g0.p[lvl];
-    int f = 0;
-    for (int k = 0; k < 4; k++) {
+  int f = 0;
+  auto put = [&](float v) {
+    buf[f & 7] = v;
+    f++;
+    if ((f & 7) == 0) st_chunk(sX, row, f - 8, Kp, buf);
+  };
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (staged) {
+      const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
+      const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
+#pragma unroll
+      for (int c = 0; c < C0; c += 4) {
+        const float4 q = *reinterpret_cast<const float4*>(src + c);
+        put(q.x);
+        put(q.y);
+        put(q.z);
+        put(q.w);
+      }
+    } else {
       const int base = G.c0[k] * C0;
+      const float* p0 = M.g0.p[lvl];
+#pragma unroll
       for (int c = 0; c < C0; c += 4) {
         const float4 q = *reinterpret_cast<const float4*>(p0 + base + c);
         float v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-          float val = v[i];
-          if (s.noise) val = val + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
-          buf[f & 7] = val;
-          f++;
+          if (s.noise) v[i] = v[i] + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
+          put(v[i]);
         }
-        if ((f & 7) == 0) st_chunk(sX, row, f - 8, Kp, buf);
       }
     }
-  } else {
-    const float* p1 = M.g1.p[lvl];
-    float acc[32];
-    for (int c = 0; c < C1; c++) acc[c] = 0.0f;
-    for (int k = 0; k < 4; k++) {
+  }
+  float acc[C1];
+#pragma unroll
+  for (int c = 0; c < C1; c++) acc[c] = 0.0f;
+  const float* foot1 = foot + f0.w * f0.h * C0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (staged) {
+      const int cy = G.c1[k] >> l1, cx = G.c1[k] & (d1 - 1);
+      const float* src = foot1 + ((cy - f1.y0) * f1.w + (cx - f1.x0)) * C1;
+#pragma unroll
+      for (int c = 0; c < C1; c += 2) {
+        const float2 q = *reinterpret_cast<const float2*>(src + c);
+        acc[c] = __fmaf_rn(G.w1[k], q.x, acc[c]);
+        acc[c + 1] = __fmaf_rn(G.w1[k], q.y, acc[c + 1]);
+      }
+    } else {
       const int base = G.c1[k] * C1;
+      const float* p1 = M.g1.p[lvl];
+#pragma unroll
       for (int c = 0; c < C1; c += 2) {
         const float2 q = *reinterpret_cast<const float2*>(p1 + base + c);
         float a = q.x, b = q.y;
@@ -146,48 +313,43 @@ __device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, con
         acc[c + 1] = __fmaf_rn(G.w1[k], b, acc[c + 1]);
       }
     }
-    int f = 4 * C0;
-    int n = 0;
-    auto put = [&](float v) {
-      buf[n++] = v;
-      if (n == 8) {
-        st_chunk(sX, row, f, Kp, buf);
-        f += 8;
-        n = 0;
-      }
-    };
-    for (int c = 0; c < C1; c++) put(acc[c]);
-    for (int i = 0; i < 12; i++) put(pos_enc(u.x, u.y, i));
-    put(s.norm_lod);
-    while (f < Kp) put(0.0f);
   }
+#pragma unroll
+  for (int c = 0; c < C1; c++) put(acc[c]);
+#pragma unroll
+  for (int i = 0; i < 12; i++) put(pos_enc(x, y, i));
+  put(s.norm_lod);
+#pragma unroll
+  for (int i = 4 * C0 + C1 + 13; i < Kp; i++) put(0.0f);
 }
 
 // Loads the fp32 master weights into the bf16 canonical tiles (zero padding past F / C).
-__device__ void load_weights(const Model& M, const TcSmem& sm, int Kp)
+template <class SH>
+__device__ void load_weights(const Model& M, uint8_t* W0, uint8_t* W1, uint8_t* Wo)
 {
-  const int F = M.F, C = M.C;
+  constexpr int F = SH::F, Kp = SH::Kp;
+  const int C = M.C;
   for (int i = threadIdx.x; i < 64 * (Kp / 8); i += kThreads) {
     const int r = i / (Kp / 8), c0 = (i % (Kp / 8)) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = (c0 + j) < F ? M.W[w0_off() + r * F + c0 + j] : 0.0f;
-    st_chunk(sm.W0, r, c0, Kp, v);
+    st_chunk(W0, r, c0, Kp, v);
   }
   for (int i = threadIdx.x; i < 64 * 8; i += kThreads) {
     const int r = i / 8, c0 = (i % 8) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = M.W[w1_off(F) + r * 64 + c0 + j];
-    st_chunk(sm.W1, r, c0, 64, v);
+    st_chunk(W1, r, c0, 64, v);
   }
   for (int i = threadIdx.x; i < 16 * 8; i += kThreads) {
     const int r = i / 8, c0 = (i % 8) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = r < C ? M.W[wo_off(F) + r * 64 + c0 + j] : 0.0f;
-    st_chunk(sm.Wo, r, c0, 64, v);
+    st_chunk(Wo, r, c0, 64, v);
   }
 }
 
-__device__ __forceinline__ double block_sum_d(double v, double* red)
+__device__ __forceinline__ double block_sum_d_tc(double v, double* red)
 {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
@@ -201,61 +363,91 @@ __device__ __forceinline__ double block_sum_d(double v, double* red)
   return r;
 }
 
-template <int KP>
+__device__ __forceinline__ void tmem_st_zero16(uint32_t taddr)
+{
+  const uint32_t z = 0;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(z));
+}
+
+template <class SH>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut out, int* __restrict__ err)
 {
+  constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp, F = SH::F;
+  constexpr uint32_t SX = SH::SX;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t tmem_base_s;
   __shared__ int fail_s;
   __shared__ double red[kThreads / 32];
+  __shared__ float u8_to_unit[256];  // v / 255 as upstream computes it (libopenntc draw_targets)
+  __shared__ CornerMasks masks_s[2];
 
-  constexpr int Kp = KP;
   const StepRec s = steps[step_idx];
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  const int row = tid & 127;       // texel row == TMEM lane
-  const int half = tid >> 7;       // column half of the epilogues
+  const int g = tid >> 7;          // group
+  const int gt = tid & 127;        // thread within group == texel row == TMEM lane
   const int quad = warp & 3;       // TMEM lane quadrant this warp may access
-  const TcSmem sm = tc_carve(smem_raw, Kp);
   const int C = M.C;
-  const int F = M.F;
+
+  uint8_t* base = smem_raw + g * GroupSmem<SH>::kBytes;
+  GroupPtrs gp;
+  gp.X = base;
+  gp.P0 = gp.X + GroupSmem<SH>::kX;
+  gp.P1 = gp.P0 + GroupSmem<SH>::kP;
+  gp.dY = gp.P1 + GroupSmem<SH>::kP;
+  gp.foot = reinterpret_cast<float*>(gp.dY + GroupSmem<SH>::kY);
+  uint8_t* sW0 = smem_raw + 2 * GroupSmem<SH>::kBytes;
+  uint8_t* sW1 = sW0 + 64 * Kp * 2;
+  uint8_t* sWo = sW1 + 64 * 64 * 2;
 
   if (tid == 0) {
-    ptx::mbar_init(&bar, 1);
+    ptx::mbar_init(&bars[0], 1);
+    ptx::mbar_init(&bars[1], 1);
     ptx::fence_mbar_init();
     fail_s = 0;
   }
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
-  load_weights(M, sm, Kp);
+  load_weights<SH>(M, sW0, sW1, sWo);
+  u8_to_unit[tid] = (float)tid / 255.0f;
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
   ptx::fence_after_sync();
   const uint32_t tbase = tmem_base_s;
-  const uint32_t lane_addr = tbase + ((uint32_t)(quad * 32) << 16);
+  const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
+  // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16)
+  for (uint32_t c = kColW0 + 16 * (uint32_t)g; c < kColWo + 16; c += 32) tmem_st_zero16(tbase + lane_off + c);
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  ptx::fence_before_sync();
+  __syncthreads();
+  ptx::fence_after_sync();
 
+  const uint32_t win = tbase + 128u * (uint32_t)g;    // this group's TMEM window (MMA address)
+  const uint32_t lwin = win + lane_off;                // ... as seen by this thread's lane
   const int ntiles = (s.texels + kTile - 1) / kTile;
   const float inv = -2.0f / ((float)C * (float)s.texels);  // libopenntc.cpp:666
   const uint8_t* target = M.package[s.lod];
+  uint64_t* bar = &bars[g];
   uint32_t phase = 0;
   double loss = 0.0;
-  bool first = true;
+  const bool issuer = gt == 0;
 
-  // one commit -> bounded wait, uniform across the CTA
   auto wait_mma = [&]() -> bool {
-    if (!ptx::mbar_wait(&bar, phase)) atomicExch(&fail_s, 1);
+    if (!ptx::mbar_wait(bar, phase)) atomicExch(&fail_s, 1);
     phase ^= 1u;
     ptx::fence_after_sync();
-    __syncthreads();
-    return fail_s == 0;
+    bar_group(g);
+    return *(volatile int*)&fail_s == 0;
   };
-  // every thread's shared-memory stores and TMEM reads done -> one thread may issue MMAs
+  // this group's shared-memory stores and TMEM reads done -> its issuer may start MMAs
   auto handoff = [&]() {
     ptx::fence_proxy_async();
     ptx::fence_before_sync();
-    __syncthreads();
+    bar_group(g);
   };
 
   constexpr uint32_t I_M128_N64_K = ptx::idesc_bf16(128, 64, false, false);
@@ -265,267 +457,316 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   constexpr uint32_t I_M64_N16_MN = ptx::idesc_bf16(64, 16, true, true);
   constexpr uint32_t I_M64_N64_MN = ptx::idesc_bf16(64, 64, true, true);
   constexpr uint32_t I_M64_NKP_MN = ptx::idesc_bf16(64, Kp, true, true);
-  const uint32_t aX = ptx::smem_addr(sm.X), aA0 = ptx::smem_addr(sm.A0), aA1 = ptx::smem_addr(sm.A1);
-  const uint32_t adY = ptx::smem_addr(sm.dY), adH1 = ptx::smem_addr(sm.dH1), adH0 = ptx::smem_addr(sm.dH0);
-  const uint32_t aW0 = ptx::smem_addr(sm.W0), aW1 = ptx::smem_addr(sm.W1), aWo = ptx::smem_addr(sm.Wo);
-  constexpr uint32_t SX = (Kp / 8) * 128;  // 8-row group stride of a [*][Kp] tile
-  constexpr uint32_t S64 = 8 * 128;        // ... of a [*][64] tile
-  constexpr uint32_t S16 = 2 * 128;        // ... of a [*][16] tile
+  const uint32_t aX = ptx::smem_addr(gp.X), aP0 = ptx::smem_addr(gp.P0), aP1 = ptx::smem_addr(gp.P1);
+  const uint32_t adY = ptx::smem_addr(gp.dY);
+  const uint32_t aW0 = ptx::smem_addr(sW0), aW1 = ptx::smem_addr(sW1), aWo = ptx::smem_addr(sWo);
 
-  for (int unit = blockIdx.x; unit < ntiles; unit += gridDim.x) {
-    // ---------------------------------------------------------------- gather
-    Unit u;
-    {
-      const int b = unit * kTile + row;
-      u.valid = b < s.texels;
-      u.x = u.y = 0;
-      if (u.valid) texel_xy(s, b, u.x, u.y);
+  for (int unit = blockIdx.x * 2 + g; unit < ntiles; unit += gridDim.x * 2) {
+    // ------------------------------------------------------------------ gather
+    const int b = unit * kTile + gt;
+    const bool valid = b < s.texels;
+    int x = 0, y = 0;
+    if (valid) texel_xy(s, b, x, y);
+    Foot f0, f1;
+    const bool staged = unit_footprint<SH>(M, s, unit, f0, f1);
+    CornerMasks& cm = masks_s[g];
+    if (staged) {
+      stage_footprint<SH>(M, s, f0, f1, gp.foot, gt);
+      for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) {
+        uint32_t* m = i < 2 * kMaxBoxW ? &cm.xlo[0][0] + i
+                      : i < 4 * kMaxBoxW ? &cm.xhi[0][0] + (i - 2 * kMaxBoxW)
+                      : i < 4 * kMaxBoxW + 2 * kMaxBoxH ? &cm.ylo[0][0] + (i - 4 * kMaxBoxW)
+                                                       : &cm.yhi[0][0] + (i - 4 * kMaxBoxW - 2 * kMaxBoxH);
+        *m = 0u;
+      }
+      bar_group(g);
+      build_masks(s, M.g0.dim[s.level], M.g1.dim[s.level], f0, f1, unit, cm, gt);
     }
-    gather_row(M, s, u, row, half, Kp, sm.X);
+    gather_row<SH>(M, s, x, y, valid, gt, staged, f0, f1, gp.foot, gp.X);
     handoff();
-    if (tid == 0) {
+    if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < Kp / 16; k++)
-        ptx::mma_bf16(tbase + kColH, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_M128_N64_K,
+        ptx::mma_bf16(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_M128_N64_K, k > 0);
+      ptx::commit(bar);
+    }
+    if (!wait_mma()) break;
+
+    // ------------------------------------------------------------------ layer 0 epilogue
+    float h0[64], h1[64];
+    ptx::ld16(lwin + 0, h0);
+    ptx::ld16(lwin + 16, h0 + 16);
+    ptx::ld16(lwin + 32, h0 + 32);
+    ptx::ld16(lwin + 48, h0 + 48);
+    ptx::ld_wait();
+#pragma unroll
+    for (int c = 0; c < 64; c += 8) {
+      float a[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) a[j] = hg_fast(h0[c + j]);
+      st_chunk(gp.P0, gt, c, 64, a);
+    }
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        ptx::mma_bf16(win, ptx::desc(aP0 + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_M128_N64_K, k > 0);
+      ptx::commit(bar);
+    }
+    if (!wait_mma()) break;
+
+    // ------------------------------------------------------------------ layer 1 epilogue
+    ptx::ld16(lwin + 0, h1);
+    ptx::ld16(lwin + 16, h1 + 16);
+    ptx::ld16(lwin + 32, h1 + 32);
+    ptx::ld16(lwin + 48, h1 + 48);
+    ptx::ld_wait();
+#pragma unroll
+    for (int c = 0; c < 64; c += 8) {
+      float a[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) a[j] = hg_fast(h1[c + j]);
+      st_chunk(gp.P1, gt, c, 64, a);
+    }
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        ptx::mma_bf16(win + 64, ptx::desc(aP1 + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_M128_N16_K,
                       k > 0);
-      ptx::commit(&bar);
+      ptx::commit(bar);
     }
     if (!wait_mma()) break;
 
-    // ---------------------------------------------------------------- layer 0 epilogue
-    float h0[32], h1[32];
+    // ------------------------------------------------------------------ output, residual, dY
     {
-      ptx::ld16(lane_addr + kColH + half * 32, h0);
-      ptx::ld16(lane_addr + kColH + half * 32 + 16, h0 + 16);
+      float yv[16], d[16];
+      ptx::ld16(lwin + 64, yv);
       ptx::ld_wait();
-      float a[8];
+      const uint8_t* tp = target + ((size_t)y * s.mip_dim + x) * C;
 #pragma unroll
-      for (int c = 0; c < 32; c += 8) {
-#pragma unroll
-        for (int j = 0; j < 8; j++) a[j] = hardgelu(h0[c + j]);
-        st_chunk(sm.A0, row, half * 32 + c, 64, a);
-      }
-    }
-    handoff();
-    if (tid == 0) {
-      ptx::fence_after_sync();
-#pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(tbase + kColH, ptx::desc(aA0 + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64),
-                      I_M128_N64_K, k > 0);
-      ptx::commit(&bar);
-    }
-    if (!wait_mma()) break;
-
-    // ---------------------------------------------------------------- layer 1 epilogue
-    {
-      ptx::ld16(lane_addr + kColH + half * 32, h1);
-      ptx::ld16(lane_addr + kColH + half * 32 + 16, h1 + 16);
-      ptx::ld_wait();
-      float a[8];
-#pragma unroll
-      for (int c = 0; c < 32; c += 8) {
-#pragma unroll
-        for (int j = 0; j < 8; j++) a[j] = hardgelu(h1[c + j]);
-        st_chunk(sm.A1, row, half * 32 + c, 64, a);
-      }
-    }
-    handoff();
-    if (tid == 0) {
-      ptx::fence_after_sync();
-#pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(tbase + kColY, ptx::desc(aA1 + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64),
-                      I_M128_N16_K, k > 0);
-      ptx::commit(&bar);
-    }
-    if (!wait_mma()) break;
-
-    // ---------------------------------------------------------------- output, residual, dY
-    {
-      float yv[8], d[8];
-      ptx::ld8(lane_addr + kColY + half * 8, yv);
-      ptx::ld_wait();
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const int c = half * 8 + j;
-        d[j] = 0.0f;
-        if (u.valid && c < C) {
-          const float tgt = (float)target[((size_t)u.y * s.mip_dim + u.x) * C + c] / 255.0f;
-          const float r = tgt - yv[j];
+      for (int c = 0; c < 16; c++) {
+        d[c] = 0.0f;
+        if (valid && c < C) {
+          const float r = u8_to_unit[tp[c]] - yv[c];
           loss += (double)r * (double)r;
-          d[j] = inv * r;
+          d[c] = inv * r;
         }
       }
-      st_chunk(sm.dY, row, half * 8, 16, d);
+      st_chunk(gp.dY, gt, 0, 16, d);
+      st_chunk(gp.dY, gt, 8, 16, d + 8);
     }
     handoff();
-    if (tid == 0) {
+    if (issuer) {
       ptx::fence_after_sync();
       // dA1 = dY Wout: B = Wout viewed [c][h] as MN-major (N = h)
-      ptx::mma_bf16(tbase + kColH, ptx::desc(adY, 128, S16), ptx::desc(aWo, S64, 128), I_M128_N64_BMN, 0);
+      ptx::mma_bf16(win, ptx::desc(adY, 128, S16), ptx::desc(aWo, S64, 128), I_M128_N64_BMN, 0);
       // dWout^T += A1^T dY : A = A1 (M = h), B = dY (N = c), K = texels
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColWo, ptx::desc(aA1 + k * 2 * S64, S64, 128), ptx::desc(adY + k * 2 * S16, S16, 128),
-                      I_M64_N16_MN, (first && k == 0) ? 0u : 1u);
-      ptx::commit(&bar);
+        ptx::mma_bf16(tbase + kColWo, ptx::desc(aP1 + k * 2 * S64, S64, 128), ptx::desc(adY + k * 2 * S16, S16, 128),
+                      I_M64_N16_MN, 1);
+      ptx::commit(bar);
     }
     if (!wait_mma()) break;
 
-    // ---------------------------------------------------------------- dH1
+    // ------------------------------------------------------------------ dH1 (into P1)
     {
-      float da[32];
-      ptx::ld16(lane_addr + kColH + half * 32, da);
-      ptx::ld16(lane_addr + kColH + half * 32 + 16, da + 16);
+      float da[64];
+      ptx::ld16(lwin + 0, da);
+      ptx::ld16(lwin + 16, da + 16);
+      ptx::ld16(lwin + 32, da + 32);
+      ptx::ld16(lwin + 48, da + 48);
       ptx::ld_wait();
-      float g[8];
 #pragma unroll
-      for (int c = 0; c < 32; c += 8) {
+      for (int c = 0; c < 64; c += 8) {
+        float gv[8];
 #pragma unroll
-        for (int j = 0; j < 8; j++) g[j] = da[c + j] * hardgelu_grad(h1[c + j]);
-        st_chunk(sm.dH1, row, half * 32 + c, 64, g);
+        for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h1[c + j]);
+        st_chunk(gp.P1, gt, c, 64, gv);
       }
     }
     handoff();
-    if (tid == 0) {
+    if (issuer) {
       ptx::fence_after_sync();
       // dA0 = dH1 W1 : B = W1 viewed [i][h] as MN-major (N = h), K = i
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(tbase + kColH, ptx::desc(adH1 + k * 256, 128, S64), ptx::desc(aW1 + k * 2 * S64, S64, 128),
-                      I_M128_N64_BMN, k > 0);
+        ptx::mma_bf16(win, ptx::desc(aP1 + k * 256, 128, S64), ptx::desc(aW1 + k * 2 * S64, S64, 128), I_M128_N64_BMN,
+                      k > 0);
       // dW1 += dH1^T A0
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW1, ptx::desc(adH1 + k * 2 * S64, S64, 128), ptx::desc(aA0 + k * 2 * S64, S64, 128),
-                      I_M64_N64_MN, (first && k == 0) ? 0u : 1u);
-      ptx::commit(&bar);
+        ptx::mma_bf16(tbase + kColW1, ptx::desc(aP1 + k * 2 * S64, S64, 128), ptx::desc(aP0 + k * 2 * S64, S64, 128),
+                      I_M64_N64_MN, 1);
+      ptx::commit(bar);
     }
     if (!wait_mma()) break;
 
-    // ---------------------------------------------------------------- dH0
+    // ------------------------------------------------------------------ dH0 (into P0)
     {
-      float da[32];
-      ptx::ld16(lane_addr + kColH + half * 32, da);
-      ptx::ld16(lane_addr + kColH + half * 32 + 16, da + 16);
+      float da[64];
+      ptx::ld16(lwin + 0, da);
+      ptx::ld16(lwin + 16, da + 16);
+      ptx::ld16(lwin + 32, da + 32);
+      ptx::ld16(lwin + 48, da + 48);
       ptx::ld_wait();
-      float g[8];
 #pragma unroll
-      for (int c = 0; c < 32; c += 8) {
+      for (int c = 0; c < 64; c += 8) {
+        float gv[8];
 #pragma unroll
-        for (int j = 0; j < 8; j++) g[j] = da[c + j] * hardgelu_grad(h0[c + j]);
-        st_chunk(sm.dH0, row, half * 32 + c, 64, g);
+        for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h0[c + j]);
+        st_chunk(gp.P0, gt, c, 64, gv);
       }
     }
     handoff();
-    if (tid == 0) {
+    if (issuer) {
       ptx::fence_after_sync();
       // dX = dH0 W0 : B = W0 viewed [h][f] as MN-major (N = f), K = h
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(tbase + kColDX, ptx::desc(adH0 + k * 256, 128, S64), ptx::desc(aW0 + k * 2 * SX, SX, 128),
-                      I_M128_NKP_BMN, k > 0);
+        ptx::mma_bf16(win, ptx::desc(aP0 + k * 256, 128, S64), ptx::desc(aW0 + k * 2 * SX, SX, 128), I_M128_NKP_BMN,
+                      k > 0);
       // dW0 += dH0^T X
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW0, ptx::desc(adH0 + k * 2 * S64, S64, 128), ptx::desc(aX + k * 2 * SX, SX, 128),
-                      I_M64_NKP_MN, (first && k == 0) ? 0u : 1u);
-      ptx::commit(&bar);
+        ptx::mma_bf16(tbase + kColW0, ptx::desc(aP0 + k * 2 * S64, S64, 128), ptx::desc(aX + k * 2 * SX, SX, 128),
+                      I_M64_NKP_MN, 1);
+      ptx::commit(bar);
     }
     if (!wait_mma()) break;
-    first = false;
 
-    // ---------------------------------------------------------------- scatter dX
-    // TMEM loads are warp-collective, so every lane loads; only valid texels scatter.
-    {
-      const bool scatter = s.grid_update && u.valid;
+    // ------------------------------------------------------------------ scatter dX
+    if (s.grid_update) {
       const int lvl = s.level;
-      Gather G;
-      if (scatter) gather_geometry(u.x, u.y, s.mip_dim, M.g0.dim[lvl], M.g1.dim[lvl], G);
-      if (half == 0) {
-        const int C0 = M.C0;
-        float* g0 = M.g0.g[lvl];
-        for (int c = 0; c < 4 * C0; c += 16) {
-          float dx[16];
-          ptx::ld16(lane_addr + kColDX + c, dx);
-          ptx::ld_wait();
-          if (scatter) {
+      const int d0 = M.g0.dim[lvl], d1 = M.g1.dim[lvl];
+      // all Kp feature-gradient columns, in 16-column aligned TMEM loads
+      float dx[Kp];
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-              const int f = c + j, k = f / C0, ch = f - k * C0;
-              atomicAdd(&g0[G.c0[k] * C0 + ch], dx[j]);
+      for (int c = 0; c < Kp; c += 16) ptx::ld16(lwin + c, dx + c);
+      ptx::ld_wait();
+      if (staged) {
+        // owner-computes: dX rows to shared memory (the group's operand tiles are free now),
+        // then each thread sums the contributions to the latent elements it owns
+        constexpr int LD = Kp + 4;
+        float* dxs = reinterpret_cast<float*>(gp.X);
+#pragma unroll
+        for (int c = 0; c < Kp; c += 4)
+          *reinterpret_cast<float4*>(dxs + gt * LD + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);
+        bar_group(g);
+        const int n0 = f0.w * f0.h * C0;
+        const int n = n0 + f1.w * f1.h * C1;
+        float* g0p = M.g0.g[lvl];
+        float* g1p = M.g1.g[lvl];
+        for (int i = gt; i < n; i += kGroupThreads) {
+          const bool first = i < n0;
+          const int j = first ? i : i - n0;
+          const int C = first ? C0 : C1;
+          const Foot& f = first ? f0 : f1;
+          const int gsel = first ? 0 : 1;
+          const int cell = j / C, ch = j - cell * C;
+          const int by = cell / f.w, bx = cell - by * f.w;
+          float sum = 0.0f;
+#pragma unroll
+          for (int kk = 0; kk < 4; kk++) {
+            const uint32_t mx = (kk & 1) ? cm.xhi[gsel][bx] : cm.xlo[gsel][bx];
+            const uint32_t my = (kk & 2) ? cm.yhi[gsel][by] : cm.ylo[gsel][by];
+            const int col = first ? kk * C0 + ch : 4 * C0 + ch;
+            for (uint32_t ym = my; ym; ym &= ym - 1) {
+              const int ty = __ffs(ym) - 1;
+              for (uint32_t xm = mx; xm; xm &= xm - 1) {
+                const int tx = __ffs(xm) - 1;
+                const float v = dxs[(ty * 16 + tx) * LD + col];
+                if (first) {
+                  sum += v;
+                } else {
+                  // the bilinear weight exactly as gather_geometry forms it
+                  const float fx = cm.fx[tx], fy = cm.fy[ty];
+                  const float w = ((kk & 1) ? fx : (1.0f - fx)) * ((kk & 2) ? fy : (1.0f - fy));
+                  sum += w * v;
+                }
+              }
             }
           }
+          if (sum != 0.0f) {
+            if (first)
+              atomicAdd(&g0p[((f0.y0 + by) * d0 + f0.x0 + bx) * C0 + ch], sum);
+            else
+              atomicAdd(&g1p[((f1.y0 + by) * d1 + f1.x0 + bx) * C1 + ch], sum);
+          }
         }
-      } else {
-        const int C0 = M.C0, C1 = M.C1;
-        float* g1 = M.g1.g[lvl];
-        float dx[32];
-        ptx::ld16(lane_addr + kColDX + 4 * C0, dx);
-        ptx::ld16(lane_addr + kColDX + 4 * C0 + 16, dx + 16);
-        ptx::ld_wait();
-        if (scatter)
-          for (int k = 0; k < 4; k++)
-            for (int c = 0; c < C1; c++) atomicAdd(&g1[G.c1[k] * C1 + c], G.w1[k] * dx[c]);
+      } else if (valid) {
+        // direct per-texel scatter (wrapped blocks, tiny tiles, oversized boxes)
+        Gather G;
+        gather_geometry(x, y, s.mip_dim, d0, d1, G);
+        float* g0p = M.g0.g[lvl];
+        float* g1p = M.g1.g[lvl];
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+          for (int c = 0; c < C0; c++) atomicAdd(&g0p[G.c0[kk] * C0 + c], dx[kk * C0 + c]);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+          for (int c = 0; c < C1; c++) atomicAdd(&g1p[G.c1[kk] * C1 + c], G.w1[kk] * dx[4 * C0 + c]);
       }
     }
     ptx::fence_before_sync();
-    __syncthreads();
+    bar_group(g);
   }
 
   // ------------------------------------------------------------------ weight gradients out
-  const double ls = block_sum_d(loss, red);
+  const double ls = block_sum_d_tc(loss, red);
   if (tid == 0) out.loss_partial[blockIdx.x] = ls;
-  if (fail_s == 0 && !first) {
-    ptx::fence_after_sync();
+  ptx::fence_after_sync();
+  if (*(volatile int*)&fail_s == 0) {
     float* dst = out.dW_partial + (size_t)blockIdx.x * M.nW;
     const int lane = tid & 31;
     const int h = quad * 16 + lane;  // M=64 accumulators: row = lane of the quadrant's first 16
-    // dW0 [64][F]: columns split between the two halves in 8-column steps
-    for (int c = half * 8; c < Kp; c += 16) {
+    const uint32_t la = tbase + lane_off;
+    for (int c = g * 8; c < Kp; c += 16) {  // dW0 [64][F], 8-column steps split by group
       float v[8];
-      ptx::ld8(lane_addr + kColW0 + c, v);
+      ptx::ld8(la + kColW0 + c, v);
       ptx::ld_wait();
       if (lane < 16)
         for (int j = 0; j < 8; j++)
           if (c + j < F) dst[w0_off() + h * F + c + j] = v[j];
     }
     {
-      float v[32];
-      ptx::ld16(lane_addr + kColW1 + half * 32, v);
-      ptx::ld16(lane_addr + kColW1 + half * 32 + 16, v + 16);
+      float v[32];  // dW1[i][h]: accumulator row i, columns h
+      ptx::ld16(la + kColW1 + g * 32, v);
+      ptx::ld16(la + kColW1 + g * 32 + 16, v + 16);
       ptx::ld_wait();
-      // accumulator row = i (dH1 column), column = h (A0 column): dW1[i][h]
       if (lane < 16)
-        for (int j = 0; j < 32; j++) dst[w1_off(F) + h * 64 + half * 32 + j] = v[j];
+        for (int j = 0; j < 32; j++) dst[w1_off(F) + h * 64 + g * 32 + j] = v[j];
     }
     {
-      float v[8];
-      ptx::ld8(lane_addr + kColWo + half * 8, v);
+      float v[8];  // dWout^T[h][c] -> dWout[c][h]
+      ptx::ld8(la + kColWo + g * 8, v);
       ptx::ld_wait();
-      // accumulator row = h, column = c: dWout[c][h]
       if (lane < 16)
-        for (int j = 0; j < 8; j++) dst[wo_off(F) + (half * 8 + j) * 64 + h] = v[j];
+        for (int j = 0; j < 8; j++) dst[wo_off(F) + (g * 8 + j) * 64 + h] = v[j];
     }
+  } else if (tid == 0) {
+    atomicExch(err, 1);
   }
-  if (fail_s != 0 && tid == 0) atomicExch(err, 1);
   ptx::fence_before_sync();
   __syncthreads();
   if (warp == 0) ptx::tmem_dealloc(tbase, kTmemCols);
 }
 
-template <int KP>
-cudaError_t launch_kp(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                      cudaStream_t stream)
+template <class SH>
+cudaError_t launch_shape(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
+                         cudaStream_t stream)
 {
-  const size_t smem = tc_smem_bytes(KP);
-  // at least 150 KB so one CTA owns an SM (and its 512 TMEM columns)
-  const size_t smem_req = smem < 150 * 1024 ? 150 * 1024 : smem;
-  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_req);
+  constexpr size_t smem = smem_bytes<SH>();
+  static_assert(smem <= 227 * 1024, "shared memory budget");
+  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tc_unit_kernel<KP><<<grid, kThreads, smem_req, stream>>>(M, d_steps, step_idx, out, d_error);
+  tc_unit_kernel<SH><<<grid, kThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error);
   return cudaGetLastError();
 }
 
@@ -542,12 +783,16 @@ int tc_max_grid()
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
                             cudaStream_t stream)
 {
-  switch (M.Fp) {
-    case 64: return launch_kp<64>(M, d_steps, step_idx, grid, out, d_error, stream);
-    case 80: return launch_kp<80>(M, d_steps, step_idx, grid, out, d_error, stream);
-    case 96: return launch_kp<96>(M, d_steps, step_idx, grid, out, d_error, stream);
-    default: return cudaErrorNotSupported;
-  }
+  // profile shapes (libopenntc.cpp:289-333): C0, C1, padded feature dim
+  if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64)
+    return launch_shape<Shape<8, 12, 64>>(M, d_steps, step_idx, grid, out, d_error, stream);
+  if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96)
+    return launch_shape<Shape<12, 20, 96>>(M, d_steps, step_idx, grid, out, d_error, stream);
+  if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80)
+    return launch_shape<Shape<12, 10, 80>>(M, d_steps, step_idx, grid, out, d_error, stream);
+  if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96)
+    return launch_shape<Shape<16, 12, 96>>(M, d_steps, step_idx, grid, out, d_error, stream);
+  return cudaErrorNotSupported;
 }
 
 }  // namespace ontc
