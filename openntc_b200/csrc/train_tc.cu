@@ -436,11 +436,13 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   double loss = 0.0;
   const bool issuer = gt == 0;
 
+  // one warp of the group polls the mbarrier; the others sleep at the group barrier
+  const bool poller = (gt >> 5) == 0;
   auto wait_mma = [&]() -> bool {
-    if (!ptx::mbar_wait(bar, phase)) atomicExch(&fail_s, 1);
+    if (poller && !ptx::mbar_wait(bar, phase)) atomicExch(&fail_s, 1);
     phase ^= 1u;
-    ptx::fence_after_sync();
     bar_group(g);
+    ptx::fence_after_sync();
     return *(volatile int*)&fail_s == 0;
   };
   // this group's shared-memory stores and TMEM reads done -> its issuer may start MMAs
@@ -657,45 +659,73 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         for (int c = 0; c < Kp; c += 4)
           *reinterpret_cast<float4*>(dxs + gt * LD + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);
         bar_group(g);
-        const int n0 = f0.w * f0.h * C0;
-        const int n = n0 + f1.w * f1.h * C1;
+        // one thread per box cell sums all channels of that cell
+        const int nc0 = f0.w * f0.h;
+        const int nc = nc0 + f1.w * f1.h;
         float* g0p = M.g0.g[lvl];
         float* g1p = M.g1.g[lvl];
-        for (int i = gt; i < n; i += kGroupThreads) {
-          const bool first = i < n0;
-          const int j = first ? i : i - n0;
-          const int C = first ? C0 : C1;
-          const Foot& f = first ? f0 : f1;
-          const int gsel = first ? 0 : 1;
-          const int cell = j / C, ch = j - cell * C;
-          const int by = cell / f.w, bx = cell - by * f.w;
-          float sum = 0.0f;
+        for (int i = gt; i < nc; i += kGroupThreads) {
+          if (i < nc0) {
+            const int by = i / f0.w, bx = i - by * f0.w;
+            float sum[C0];
 #pragma unroll
-          for (int kk = 0; kk < 4; kk++) {
-            const uint32_t mx = (kk & 1) ? cm.xhi[gsel][bx] : cm.xlo[gsel][bx];
-            const uint32_t my = (kk & 2) ? cm.yhi[gsel][by] : cm.ylo[gsel][by];
-            const int col = first ? kk * C0 + ch : 4 * C0 + ch;
-            for (uint32_t ym = my; ym; ym &= ym - 1) {
-              const int ty = __ffs(ym) - 1;
-              for (uint32_t xm = mx; xm; xm &= xm - 1) {
-                const int tx = __ffs(xm) - 1;
-                const float v = dxs[(ty * 16 + tx) * LD + col];
-                if (first) {
-                  sum += v;
-                } else {
-                  // the bilinear weight exactly as gather_geometry forms it
-                  const float fx = cm.fx[tx], fy = cm.fy[ty];
-                  const float w = ((kk & 1) ? fx : (1.0f - fx)) * ((kk & 2) ? fy : (1.0f - fy));
-                  sum += w * v;
+            for (int c = 0; c < C0; c++) sum[c] = 0.0f;
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+              const uint32_t mx = (kk & 1) ? cm.xhi[0][bx] : cm.xlo[0][bx];
+              const uint32_t my = (kk & 2) ? cm.yhi[0][by] : cm.ylo[0][by];
+              for (uint32_t ym = my; ym; ym &= ym - 1) {
+                const int ty = __ffs(ym) - 1;
+                for (uint32_t xm = mx; xm; xm &= xm - 1) {
+                  const float* src = dxs + ((ty << 4) + __ffs(xm) - 1) * LD + kk * C0;
+#pragma unroll
+                  for (int c = 0; c < C0; c += 4) {
+                    const float4 v = *reinterpret_cast<const float4*>(src + c);
+                    sum[c] += v.x;
+                    sum[c + 1] += v.y;
+                    sum[c + 2] += v.z;
+                    sum[c + 3] += v.w;
+                  }
                 }
               }
             }
-          }
-          if (sum != 0.0f) {
-            if (first)
-              atomicAdd(&g0p[((f0.y0 + by) * d0 + f0.x0 + bx) * C0 + ch], sum);
-            else
-              atomicAdd(&g1p[((f1.y0 + by) * d1 + f1.x0 + bx) * C1 + ch], sum);
+            float* dst = g0p + ((f0.y0 + by) * d0 + f0.x0 + bx) * C0;
+#pragma unroll
+            for (int c = 0; c < C0; c++)
+              if (sum[c] != 0.0f) atomicAdd(dst + c, sum[c]);
+          } else {
+            const int j = i - nc0;
+            const int by = j / f1.w, bx = j - by * f1.w;
+            float sum[C1];
+#pragma unroll
+            for (int c = 0; c < C1; c++) sum[c] = 0.0f;
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+              const uint32_t mx = (kk & 1) ? cm.xhi[1][bx] : cm.xlo[1][bx];
+              const uint32_t my = (kk & 2) ? cm.yhi[1][by] : cm.ylo[1][by];
+              for (uint32_t ym = my; ym; ym &= ym - 1) {
+                const int ty = __ffs(ym) - 1;
+                const float fy = cm.fy[ty];
+                const float wy = (kk & 2) ? fy : (1.0f - fy);
+                for (uint32_t xm = mx; xm; xm &= xm - 1) {
+                  const int tx = __ffs(xm) - 1;
+                  const float fx = cm.fx[tx];
+                  // the bilinear weight exactly as gather_geometry forms it
+                  const float w = ((kk & 1) ? fx : (1.0f - fx)) * wy;
+                  const float* src = dxs + ((ty << 4) + tx) * LD + 4 * C0;
+#pragma unroll
+                  for (int c = 0; c < C1; c += 2) {
+                    const float2 v = *reinterpret_cast<const float2*>(src + c);
+                    sum[c] += w * v.x;
+                    sum[c + 1] += w * v.y;
+                  }
+                }
+              }
+            }
+            float* dst = g1p + ((f1.y0 + by) * d1 + f1.x0 + bx) * C1;
+#pragma unroll
+            for (int c = 0; c < C1; c++)
+              if (sum[c] != 0.0f) atomicAdd(dst + c, sum[c]);
           }
         }
       } else if (valid) {
