@@ -160,8 +160,9 @@ def run_ours(args):
     assert r == ont.Result.Success, r
     assert ctx.load_manifest(manifest) == ont.Result.Success
     precision = ont.Precision.BF16 if args.precision == "bf16" else ont.Precision.FP32
+    latent_adam = ont.LatentAdam.DENSE if args.latent_adam == "dense" else ont.LatentAdam.DEFERRED
     ctx.begin_training(ont.Quality.Low, WORKLOAD["grids_per_batch"], steps=WORKLOAD["schedule_steps"],
-                       precision=precision)
+                       precision=precision, latent_adam=latent_adam)
     K, W = args.steps, args.warmup
     assert W + 3 * K + 1 < int(0.95 * WORKLOAD["schedule_steps"]), "timed steps must stay before the latent lock"
     B = WORKLOAD["batch_texels"]
@@ -216,26 +217,48 @@ def run_ours(args):
     ctx._lib.ontc_profile_kernels(ctx.handle, 0)
     pk = peaks()
     adam = kt[_abi.KCLASS_ADAM]
+    catchup = kt[_abi.KCLASS_CATCHUP]
     units = kt[_abi.KCLASS_UNITS_BF16 if precision == ont.Precision.BF16 else _abi.KCLASS_UNITS_FP32]
     if units.launches == 0:
         units = kt[_abi.KCLASS_UNITS_FP32]
-    step_ms_prof = (adam.total_ms + units.total_ms) / max(1, adam.launches)
-    adam_gbs = adam.bytes / (adam.total_ms / 1e3) / 1e9 if adam.total_ms > 0 else 0.0
-    units_tflops = units.flops / (units.total_ms / 1e3) / 1e12 if units.total_ms > 0 else 0.0
-    traffic = None
+    step_ms_prof = (adam.total_ms + units.total_ms + catchup.total_ms) / K
+    traffic_tab = {}
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("adam_step_bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "adam_step_kernel (fused latent Adam/clamp/zero + decoder Adam)",
-                "achieved": round(adam_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": round(adam_gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"],
-                "traffic": traffic, "algorithmic_bytes_per_launch": adam.bytes / max(1, adam.launches),
-                "avg_launch_us": 1e3 * adam.total_ms / max(1, adam.launches),
-                "share_of_step": round(adam.total_ms / max(1e-9, adam.total_ms + units.total_ms), 3),
-                "mlp_kernel": {"name": "fused tile kernel (gather/MLP fwd+bwd/scatter)",
-                               "achieved_tflops": round(units_tflops, 2), "peak_tflops": pk["bf16_tflops"],
-                               "frac": round(units_tflops / pk["bf16_tflops"], 4),
-                               "avg_launch_us": 1e3 * units.total_ms / max(1, units.launches)}}
+        traffic_tab = json.loads(tfile.read_text())
+
+    def per_launch(k):
+        return 1e3 * k.total_ms / max(1, k.launches)
+
+    def gbs(k):
+        return k.bytes / (k.total_ms / 1e3) / 1e9 if k.total_ms > 0 else 0.0
+
+    units_tflops = units.flops / (units.total_ms / 1e3) / 1e12 if units.total_ms > 0 else 0.0
+    step_total = max(1e-9, adam.total_ms + units.total_ms + catchup.total_ms)
+    kernels = {
+        "tile": {"name": "fused tile kernel (gather/MLP fwd+bwd/scatter)", "bound": "tensor",
+                 "achieved": round(units_tflops, 2), "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                 "algorithmic_flops_per_launch": units.flops / max(1, units.launches),
+                 "avg_launch_us": per_launch(units), "share_of_step": round(units.total_ms / step_total, 3),
+                 "traffic": traffic_tab.get("tile_bytes_per_launch")},
+        "adam": {"name": "adam_step_kernel (decoder Adam + footprint latent Adam/clamp/zero)", "bound": "hbm",
+                 "achieved": round(gbs(adam), 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                 "algorithmic_bytes_per_launch": adam.bytes / max(1, adam.launches),
+                 "avg_launch_us": per_launch(adam), "share_of_step": round(adam.total_ms / step_total, 3),
+                 "traffic": traffic_tab.get("adam_step_bytes_per_launch")},
+        "catchup": {"name": "catchup_kernel + sweep_kernel (zero-gradient replay)", "bound": "hbm",
+                    "achieved": round(gbs(catchup), 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "launches_per_step": catchup.launches / K, "avg_launch_us": per_launch(catchup),
+                    "share_of_step": round(catchup.total_ms / step_total, 3), "traffic": None},
+    }
+    for k in kernels.values():
+        k["frac"] = round(k["achieved"] / k["peak"], 4) if k["peak"] else None
+    dominant = max(("tile", "adam", "catchup"), key=lambda n: kernels[n]["share_of_step"])
+    d = kernels[dominant]
+    roofline = {"bound": d["bound"], "kernel": d["name"], "achieved": d["achieved"], "peak": d["peak"],
+                "unit": d["unit"], "frac": d["frac"], "peak_src": pk["src"], "traffic": d["traffic"],
+                "avg_launch_us": d["avg_launch_us"], "share_of_step": d["share_of_step"],
+                "kernels": kernels}
 
     out = None
     if rank == 0:
@@ -248,7 +271,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic: seeded 2048^2 9-channel PBR set (value-noise height, ramp albedo, normals, "
                     "roughness, metallic, AO), one material per rank",
-            "config": dict(WORKLOAD, precision=args.precision, l2=L2_NOTE,
+            "config": dict(WORKLOAD, precision=args.precision, latent_adam=args.latent_adam, l2=L2_NOTE,
                            parallelism=f"replicas x{world} (independent materials, no collective)"),
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -321,6 +344,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
+    ap.add_argument("--latent-adam", choices=["deferred", "dense"], default="deferred")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     assert args.warmup >= 3

@@ -156,8 +156,18 @@ typedef struct ontc_train_options {
   int32_t lock_step;
   int32_t precision;      /* ONTC_PRECISION_* */
   int32_t noise_mode;     /* ONTC_NOISE_* */
-  int32_t reserved[3];
+  int32_t latent_adam;    /* ONTC_LATENT_ADAM_* */
+  int32_t reserved[2];
 } ontc_train_options;
+
+/* How the latent Adam update of upstream (libopenntc.cpp:755-790: every latent of the step's
+ * level, every step) is carried out.  Both give the same values.
+ *   DEFERRED (default): only the latents a step touches are updated in the step; the
+ *                       zero-gradient steps the others miss are replayed (same arithmetic)
+ *                       before they are next read, in level sweeps, at the lock and before
+ *                       ontc_train returns.
+ *   DENSE:              one pass over the whole level every step. */
+enum { ONTC_LATENT_ADAM_DEFERRED = 0, ONTC_LATENT_ADAM_DENSE = 1 };
 
 /* Quantisation-noise surrogate used before the latent lock.
  *   COUNTER (default): U(-delta/2, delta/2) from a counter-based hash of (step, element),
@@ -241,7 +251,8 @@ enum {
   ONTC_KCLASS_UNITS_FP32 = 0, /* fused gather/MLP/backward/scatter tile kernel, fp32 SIMT */
   ONTC_KCLASS_UNITS_BF16 = 1, /* the same, tcgen05 bf16 */
   ONTC_KCLASS_ADAM = 2,       /* fused decoder + latent Adam / clamp / gradient-zero pass */
-  ONTC_KCLASS_COUNT = 3
+  ONTC_KCLASS_CATCHUP = 3,    /* deferred optimiser: footprint catch-up and level sweeps */
+  ONTC_KCLASS_COUNT = 4
 };
 typedef struct ontc_kernel_time {
   int64_t launches;

@@ -77,6 +77,11 @@ int ontc_debug_package(ontc_context* ctx, int32_t mip, uint8_t* out);
 /* Geometry: [F, Fp, C, mips, levels, nW, g0_dim[6], g1_dim[6], mip_dim[12], batch_i, lock_i, batch_count] */
 int ontc_debug_shape(ontc_context* ctx, int32_t* out32);
 
+/* The deferred optimiser's footprint cover (host code, no device): n half-open rectangles
+ * in[k] = {x0, y0, x1, y1} -> disjoint rectangles with the same union in out (4 ints each).
+ * Returns their count, or -1 when more than cap are needed. */
+int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,11 @@ class Precision(enum.IntEnum):
     FP32 = 1
 
 
+class LatentAdam(enum.IntEnum):
+    DEFERRED = 0  # footprint updates + exact replay of the zero-gradient steps
+    DENSE = 1     # one pass over the whole level every step
+
+
 class NoiseMode(enum.IntEnum):
     COUNTER = 0   # counter-based surrogate, generated at the touched latents only
     UPSTREAM = 1  # upstream's cuRAND stream and level-wide buffers (trajectory parity)
@@ -118,7 +123,7 @@ class Context:
 
     def begin_training(self, quality: int, grids_per_batch: int = 1, steps: int | None = None,
                        lock_step: int | None = None, precision: int = Precision.BF16,
-                       noise_mode: int = NoiseMode.COUNTER):
+                       noise_mode: int = NoiseMode.COUNTER, latent_adam: int = LatentAdam.DEFERRED):
         self._lib.ontc_begin_training(self._h, int(quality), int(grids_per_batch))
         o = TrainOptions()
         o.steps_override = steps or 0
@@ -126,6 +131,7 @@ class Context:
         o.lock_step = lock_step or 0
         o.precision = int(precision)
         o.noise_mode = int(noise_mode)
+        o.latent_adam = int(latent_adam)
         r = self._lib.ontc_set_train_options(self._h, C.byref(o))
         if r != 0:
             raise RuntimeError(f"ontc_set_train_options: {Result(r).name}")

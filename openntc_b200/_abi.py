@@ -77,7 +77,11 @@ class TextureData(C.Structure):
 
 class TrainOptions(C.Structure):
     _fields_ = [("steps_override", C.c_int32), ("has_lock_step", C.c_int32), ("lock_step", C.c_int32),
-                ("precision", C.c_int32), ("noise_mode", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("precision", C.c_int32), ("noise_mode", C.c_int32), ("latent_adam", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
+
+
+LATENT_ADAM_DEFERRED, LATENT_ADAM_DENSE = 0, 1
 
 
 NOISE_COUNTER, NOISE_UPSTREAM = 0, 1
@@ -87,7 +91,7 @@ class KernelTime(C.Structure):
     _fields_ = [("launches", C.c_int64), ("total_ms", C.c_double), ("bytes", C.c_double), ("flops", C.c_double)]
 
 
-KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_COUNT = 0, 1, 2, 3
+KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_CATCHUP, KCLASS_COUNT = 0, 1, 2, 3, 4
 
 
 class DebugStep(C.Structure):
@@ -143,6 +147,7 @@ SIGNATURES = {
     "ontc_debug_lanczos_weights": (C.c_int, [C.c_void_p]),
     "ontc_debug_package": (C.c_int, [P, C.c_int32, C.c_void_p]),
     "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
+    "ontc_debug_disjoint_cover": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
 }
 
 

@@ -38,8 +38,24 @@ struct StepRec {
   float gb1, gb2;       // latent Adam bias factors (per-level step counter)
   int32_t ox[kMaxGrids], oy[kMaxGrids];
   int32_t step;         // global step index (batch_i_)
-  int32_t pad[3];
+  int32_t gstep;        // step index within the level (grid_batch_i_ before the step)
+  int32_t gfloor;       // deferred optimiser: every latent of the level has had >= gfloor steps
+  int32_t sweep_from;   // host only: floor before the level sweep that precedes this step, or -1
 };
+
+// Latent cells a step can touch, as DISJOINT rectangles per pyramid: the union of every
+// tile's cell range (texel ranges that wrap around the mip edge split in two per axis),
+// conservative by one cell.  Each cell of the footprint belongs to exactly one rectangle, so
+// the deferred latent optimiser can give every one its own thread with no claiming.
+constexpr int kMaxFootRects = 40;
+struct FootRec {
+  int32_t n[2];                     // rectangles per pyramid
+  int32_t cells[2];                 // cells over the rectangles
+  int32_t start[2][kMaxFootRects];  // first cell of each rectangle within its pyramid
+  int16_t r[2][kMaxFootRects][4];   // x0, y0, w, h in cells
+};
+
+constexpr int kHistRing = 64;  // level steps a latent cell may lag behind its level
 
 // One latent pyramid (g0 or g1), fp32 master copy plus Adam state, [dim][dim][C] row-major
 // per level, exactly upstream's layout (ntc_kernel.cu:127-129).
@@ -68,6 +84,10 @@ struct Model {
   // upstream-compatible noise buffers (StepRec::noise == 2), indexed like the level's latents
   const float* noise0;
   const float* noise1;
+  // deferred latent optimiser: level steps applied per cell, and the per-level ring of
+  // (lr, bias1, bias2) of the level's recent steps
+  int32_t* applied[2][kMaxLevels];
+  float4* hist[kMaxLevels];
 };
 
 ONTC_HD int w0_off() { return 0; }

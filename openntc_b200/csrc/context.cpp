@@ -146,6 +146,10 @@ struct ontc_context {
   int32_t grid_batch_i[ONTC_MAX_LEVELS] = {};
   int32_t precision = ONTC_PRECISION_BF16;
   int32_t noise_mode = ONTC_NOISE_COUNTER;
+  int32_t optimizer = ONTC_LATENT_ADAM_DEFERRED;
+  int32_t upd_count[ONTC_MAX_LEVELS] = {};  // level steps with a latent update (before the lock)
+  int32_t swept[ONTC_MAX_LEVELS] = {};      // every cell of the level has received this many
+  int32_t lock_from[ONTC_MAX_LEVELS] = {}, lock_to[ONTC_MAX_LEVELS] = {};  // sweeps at the lock
   uint32_t last_seed = 0;
   bool last_noise = false;
   std::mt19937 gen{123};
@@ -159,6 +163,9 @@ struct ontc_context {
   DBuf<float> W, Wm, Wv, dWpart, calib;
   DBuf<double> loss_part, losses, eval_sums;
   DBuf<StepRec> steps, aux_steps;
+  DBuf<int32_t> applied[2][ONTC_MAX_LEVELS];
+  DBuf<float4> hist;
+  FootRec* h_foots = nullptr;  // pinned staging
   DBuf<uint8_t> package[ONTC_MAX_MIPS];
   DBuf<uint32_t> packbuf;
   DBuf<int> tc_error;
@@ -252,6 +259,11 @@ struct ontc_context {
     M.nW = nW;
     M.noise0 = noise_buf[0].p;
     M.noise1 = noise_buf[1].p;
+    for (int l = 0; l < levels; l++) {
+      M.applied[0][l] = applied[0][l].p;
+      M.applied[1][l] = applied[1][l].p;
+      M.hist[l] = hist.p ? hist.p + (size_t)l * kHistRing : nullptr;
+    }
     return M;
   }
 
@@ -276,11 +288,159 @@ bool ensure_host_steps(ontc_context* c, size_t n)
 {
   if (c->h_steps_cap >= n) return true;
   if (c->h_steps) cudaFreeHost(c->h_steps);
+  if (c->h_foots) cudaFreeHost(c->h_foots);
   c->h_steps = nullptr;
+  c->h_foots = nullptr;
   c->h_steps_cap = 0;
   if (cudaMallocHost(&c->h_steps, n * sizeof(StepRec)) != cudaSuccess) return false;
+  if (cudaMallocHost(&c->h_foots, n * sizeof(FootRec)) != cudaSuccess) return false;
   c->h_steps_cap = n;
   return true;
+}
+
+// Cell ranges of one pyramid touched by texel range [o, o + T) of a D-wide mip (wrapping),
+// with a one-cell margin: the corner cells come from gather_geometry's arithmetic.
+void foot_ranges(int o, int T, int D, int gd, int out[2][2], int& n)
+{
+  auto cells = [&](int a, int b, int* r) {
+    const float rm = 1.0f / (float)D;  // exact: D is a power of two
+    const int lo = (int)std::floor(((float)a + 0.5f) * rm * (float)gd - 0.5f);
+    const int hi = (int)std::floor(((float)b + 0.5f) * rm * (float)gd - 0.5f) + 1;
+    r[0] = std::clamp(lo - 1, 0, gd - 1);
+    r[1] = std::clamp(hi + 1, 0, gd - 1);
+  };
+  if (T >= D) {
+    cells(0, D - 1, out[0]);
+    n = 1;
+  } else if (o + T <= D) {
+    cells(o, o + T - 1, out[0]);
+    n = 1;
+  } else {
+    cells(o, D - 1, out[0]);
+    cells(0, o + T - 1 - D, out[1]);
+    n = 2;
+  }
+}
+
+// Disjoint cover of the union of half-open rectangles in[k] = {x0, y0, x1, y1}: elementary
+// cells between consecutive distinct edges, runs of covered cells merged along x within each
+// band, runs identical to the previous band's merged along y.  Returns the count, or -1 past cap.
+int disjoint_cover(const int (*in)[4], int n, int (*out)[4], int cap)
+{
+  std::vector<int> xs, ys;
+  for (int k = 0; k < n; k++) {
+    xs.push_back(in[k][0]);
+    xs.push_back(in[k][2]);
+    ys.push_back(in[k][1]);
+    ys.push_back(in[k][3]);
+  }
+  std::sort(xs.begin(), xs.end());
+  xs.erase(std::unique(xs.begin(), xs.end()), xs.end());
+  std::sort(ys.begin(), ys.end());
+  ys.erase(std::unique(ys.begin(), ys.end()), ys.end());
+  struct Open { int ix0, ix1, band, out; };
+  std::vector<Open> open;
+  int m = 0;
+  for (size_t iy = 0; iy + 1 < ys.size(); iy++) {
+    size_t ix = 0;
+    while (ix + 1 < xs.size()) {
+      auto covered = [&](size_t i) {
+        for (int k = 0; k < n; k++)
+          if (in[k][0] <= xs[i] && xs[i + 1] <= in[k][2] && in[k][1] <= ys[iy] && ys[iy + 1] <= in[k][3]) return true;
+        return false;
+      };
+      if (!covered(ix)) {
+        ix++;
+        continue;
+      }
+      size_t ix1 = ix + 1;
+      while (ix1 + 1 < xs.size() && covered(ix1)) ix1++;
+      bool extended = false;
+      for (Open& o : open)
+        if (o.band == (int)iy - 1 && o.ix0 == (int)ix && o.ix1 == (int)ix1) {
+          out[o.out][3] = ys[iy + 1];
+          o.band = (int)iy;
+          extended = true;
+          break;
+        }
+      if (!extended) {
+        if (m >= cap) return -1;
+        out[m][0] = xs[ix];
+        out[m][1] = ys[iy];
+        out[m][2] = xs[ix1];
+        out[m][3] = ys[iy + 1];
+        open.push_back({(int)ix, (int)ix1, (int)iy, m});
+        m++;
+      }
+      ix = ix1;
+    }
+  }
+  return m;
+}
+
+// The footprint of a step (FootRec, common.cuh): per pyramid the disjoint cover of every
+// tile's cell rectangles, or the whole level when the cover needs too many rectangles.
+void make_foot(const ontc_context* c, const StepRec& s, FootRec& F)
+{
+  F = FootRec();
+  for (int g = 0; g < 2; g++) {
+    const int gd = g == 0 ? c->g0_dim[s.level] : c->g1_dim[s.level];
+    int in[4 * kMaxGrids][4], out[kMaxFootRects][4], n = 0;
+    for (int t = 0; t < s.n_grids; t++) {
+      int xr[2][2], yr[2][2], nx, ny;
+      foot_ranges(s.ox[t], s.tile_dim, s.mip_dim, gd, xr, nx);
+      foot_ranges(s.oy[t], s.tile_dim, s.mip_dim, gd, yr, ny);
+      for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+          in[n][0] = xr[i][0];
+          in[n][1] = yr[j][0];
+          in[n][2] = xr[i][1] + 1;
+          in[n][3] = yr[j][1] + 1;
+          n++;
+        }
+    }
+    int m = disjoint_cover(in, n, out, kMaxFootRects);
+    if (m < 0) {
+      out[0][0] = out[0][1] = 0;
+      out[0][2] = out[0][3] = gd;
+      m = 1;
+    }
+    int cells = 0;
+    for (int k = 0; k < m; k++) {
+      F.r[g][k][0] = (int16_t)out[k][0];
+      F.r[g][k][1] = (int16_t)out[k][1];
+      F.r[g][k][2] = (int16_t)(out[k][2] - out[k][0]);
+      F.r[g][k][3] = (int16_t)(out[k][3] - out[k][1]);
+      F.start[g][k] = cells;
+      cells += (out[k][2] - out[k][0]) * (out[k][3] - out[k][1]);
+    }
+    F.n[g] = m;
+    F.cells[g] = cells;
+  }
+}
+
+// Brings every latent of every level from level step from[l] up to to[l] (deferred optimiser).
+cudaError_t sweep_levels(ontc_context* c, const int32_t* from, const int32_t* to)
+{
+  const Model M = c->model();
+  for (int l = 0; l < c->levels; l++) {
+    if (to[l] <= from[l]) continue;
+    c->prof_begin();
+    cudaError_t e = launch_sweep(M, l, from[l], to[l], c->stream);
+    c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, l) + c->level_elems(1, l)), 0.0);
+    c->launches++;
+    if (e) return e;
+  }
+  return cudaSuccess;
+}
+
+// Brings every latent of every level up to its level's step count (deferred optimiser).
+cudaError_t flush_latents(ontc_context* c)
+{
+  if (c->optimizer != ONTC_LATENT_ADAM_DEFERRED) return cudaSuccess;
+  cudaError_t e = sweep_levels(c, c->swept, c->upd_count);
+  for (int l = 0; l < c->levels; l++) c->swept[l] = c->upd_count[l];
+  return e;
 }
 
 // Full-mip "step" used by Eval and Calibrate: every texel of the mip once.
@@ -312,6 +472,9 @@ void unload(ontc_context* c)
   c->losses.release();
   c->noise_buf[0].release();
   c->noise_buf[1].release();
+  for (int g = 0; g < 2; g++)
+    for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->applied[g][l].release();
+  c->hist.release();
   c->g0_host_packed.clear();
   c->g1_host_packed.clear();
   for (int i = 0; i < ONTC_MAX_LEVELS; i++) c->g0_host[i] = c->g1_host[i] = nullptr;
@@ -443,6 +606,7 @@ void ontc_destroy(ontc_context* c)
   if (!c) return;
   unload(c);
   if (c->h_steps) cudaFreeHost(c->h_steps);
+  if (c->h_foots) cudaFreeHost(c->h_foots);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -610,7 +774,11 @@ int ontc_load_manifest(ontc_context* c, const char* path)
     }
     words0 += c->level_elems(0, l) * c->b0 / 32;
     words1 += c->level_elems(1, l) * c->b1 / 32;
+    if (c->applied[0][l].alloc((size_t)c->g0_dim[l] * c->g0_dim[l]) ||
+        c->applied[1][l].alloc((size_t)c->g1_dim[l] * c->g1_dim[l]))
+      return fail(ONTC_ALLOCATION_FAILURE);
   }
+  if (c->hist.alloc((size_t)c->levels * kHistRing)) return fail(ONTC_ALLOCATION_FAILURE);
   if (c->packbuf.alloc(std::max(c->level_elems(0, 0) * c->b0 / 32, c->level_elems(1, 0) * c->b1 / 32) + 4))
     return fail(ONTC_ALLOCATION_FAILURE);
   c->g0_host_packed.assign(words0, 0);
@@ -705,7 +873,8 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
   c->lock_i = (95 * c->batch_count) / 100;
   c->batch_i = 0;
   c->grids = std::clamp(grids_per_batch, 1, kMaxGrids);
-  for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->grid_batch_i[l] = 0;
+  for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->grid_batch_i[l] = c->upd_count[l] = c->swept[l] = 0;
+  if (!deferred_supported(c->C0, c->C1)) c->optimizer = ONTC_LATENT_ADAM_DENSE;
   c->last_noise = false;
 
   cudaError_t e = cudaSuccess;
@@ -720,6 +889,7 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
       if (!e) e = cudaMemset(c->lat[g][1][l].p, 0, n * sizeof(float));
       if (!e) e = cudaMemset(c->lat[g][2][l].p, 0, n * sizeof(float));
       if (!e) e = cudaMemset(c->lat[g][3][l].p, 0, n * sizeof(float));
+      if (!e) e = cudaMemset(c->applied[g][l].p, 0, c->applied[g][l].n * sizeof(int32_t));
     }
   }
   // Kaiming-uniform, bound 1/sqrt(fan_in) (libopenntc.cpp:60-78): W0 [64][F], W1 [64][64], Wout [16][64]
@@ -757,6 +927,9 @@ int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
   }
   if (o->has_lock_step) c->lock_i = std::max(0, o->lock_step);
   if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
+  if (o->latent_adam != ONTC_LATENT_ADAM_DEFERRED && o->latent_adam != ONTC_LATENT_ADAM_DENSE) return ONTC_INVALID_STATE;
+  // the deferred kernels are compiled per profile channel pair; anything else runs dense
+  c->optimizer = deferred_supported(c->C0, c->C1) ? o->latent_adam : ONTC_LATENT_ADAM_DENSE;
   c->noise_mode = o->noise_mode;
   if (c->noise_mode == ONTC_NOISE_UPSTREAM) {
     if (!c->manifest_loaded) return ONTC_INVALID_STATE;
@@ -839,6 +1012,28 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       s.gb1 = 1.0f / (1.0f - powf(0.9f, c->grid_batch_i[s.level] + 1.0f));
       s.gb2 = 1.0f / (1.0f - powf(0.999f, c->grid_batch_i[s.level] + 1.0f));
       c->grid_batch_i[s.level] += 1;
+      // deferred optimiser bookkeeping, in step order: the floor each level is swept to
+      s.gstep = c->upd_count[s.level];
+      s.gfloor = 0;
+      s.sweep_from = -1;
+      if (bi == c->lock_i && c->optimizer == ONTC_LATENT_ADAM_DEFERRED)
+        for (int l = 0; l < c->levels; l++) {
+          c->lock_from[l] = c->swept[l];
+          c->lock_to[l] = c->upd_count[l];
+          c->swept[l] = c->upd_count[l];
+        }
+      if (s.grid_update) {
+        c->upd_count[s.level] += 1;
+        if (c->optimizer == ONTC_LATENT_ADAM_DEFERRED) {
+          // a cell may lag its level by at most kHistRing steps (the ring of step scalars)
+          if (s.gstep - c->swept[s.level] >= kHistRing) {
+            s.sweep_from = c->swept[s.level];
+            c->swept[s.level] = s.gstep;
+          }
+          s.gfloor = c->swept[s.level];
+          make_foot(c, s, c->h_foots[k]);
+        }
+      }
       s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
       s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
       s.step = bi;
@@ -856,6 +1051,7 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       }
       if (bi == c->lock_i) {
         // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
+        if (!e && c->optimizer == ONTC_LATENT_ADAM_DEFERRED) e = sweep_levels(c, c->lock_from, c->lock_to);
         for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
           e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
           if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
@@ -863,6 +1059,22 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
         }
         for (int g = 0; g < 2 && e == cudaSuccess; g++)
           if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
+      }
+      const bool deferred = c->optimizer == ONTC_LATENT_ADAM_DEFERRED && s.grid_update;
+      const FootRec& fr = c->h_foots[k];
+      if (deferred) {
+        if (s.sweep_from >= 0) {
+          c->prof_begin();
+          if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
+          c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)),
+                      0.0);
+          c->launches++;
+        }
+        c->prof_begin();
+        if (!e) e = launch_catchup(M, c->steps.p, k, fr, c->stream);
+        // reads and writes p, m, v of the footprint latents that lag
+        c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
+        c->launches++;
       }
       const int units = (s.texels + kTile - 1) / kTile;
       TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
@@ -886,10 +1098,19 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
       c->launches++;
       c->prof_begin();
-      if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
-      // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
-      c->prof_end(ONTC_KCLASS_ADAM,
-                  s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0, 0.0);
+      if (deferred) {
+        if (!e)
+          e = launch_footprint_update(M, c->steps.p, k, fr, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
+                                      c->stream);
+        // footprint latents: p, m, v, g in and out (32 B each)
+        c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
+      } else {
+        if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
+        // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
+        c->prof_end(ONTC_KCLASS_ADAM,
+                    s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
+                    0.0);
+      }
       c->launches++;
       c->last_seed = s.seed;
       c->last_noise = s.noise != 0;
@@ -897,6 +1118,8 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
       c->batch_i = bi + 1;
     }
   }
+  // every latent is current whenever control returns to the caller
+  if (!e) e = flush_latents(c);
   if (!e) e = cudaStreamSynchronize(c->stream);
   if (!e && tc_failed(c)) e = cudaErrorLaunchTimeout;
   if (e != cudaSuccess) {
@@ -1232,6 +1455,12 @@ int ontc_debug_package(ontc_context* c, int32_t mip, uint8_t* out)
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!e) e = cudaMemcpy(out, c->package[mip].p, c->package[mip].n, cudaMemcpyDeviceToHost);
   return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap)
+{
+  if (n < 0 || cap < 0 || (n > 0 && (!in || !out))) return -1;
+  return disjoint_cover(reinterpret_cast<const int (*)[4]>(in), n, reinterpret_cast<int (*)[4]>(out), cap);
 }
 
 int ontc_debug_shape(ontc_context* c, int32_t* o)

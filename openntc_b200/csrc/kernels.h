@@ -31,6 +31,18 @@ int tc_max_grid();
 // of the step's level, one launch.  Also reduces the loss partials into loss_out[step].
 cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, const float* dW_partial,
                              const double* loss_partial, int grid, double* loss_out, cudaStream_t stream);
+// deferred latent optimiser (see optim.cu): catch the step's footprint up to its level step,
+// apply the step's gradient to the footprint (plus the decoder Adam), sweep a whole level
+cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+                           cudaStream_t stream);
+// decoder Adam + loss reduction + the step's gradient on its footprint, one launch
+cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+                                    const float* dW_partial, const double* loss_partial, int grid,
+                                    double* loss_out, cudaStream_t stream);
+// every latent of `level` from level step max(applied, from) to J
+cudaError_t launch_sweep(const Model& M, int level, int from, int J, cudaStream_t stream);
+// whether the deferred kernels are compiled for this (C0, C1) pair
+bool deferred_supported(int c0, int c1);
 // upstream quantize_grid over one latent tensor (ntc_kernel.cu:448-460)
 cudaError_t launch_quantize_grid(float* g, long long n, int bits, float delta, cudaStream_t stream);
 // upstream quantize_pack (ntc_kernel.cu:486-499), n*bits must be a multiple of 32

@@ -8,6 +8,8 @@
 //    HBM-bound: 16 B read + 16 B written per latent.
 //  * quantize_grid / quantize_pack: upstream's lock-step snap and final code packing
 //    (ntc_kernel.cu:448-507), integer-exact.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -57,6 +59,211 @@ __device__ __forceinline__ void adam_latent4(float* __restrict__ P, float* __res
   *reinterpret_cast<float4*>(G + i) = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+constexpr int kDecWarps = 8;  // warps of a decoder CTA, each summing every 8th partial
+
+// Decoder Adam for 32 weights (CTA `blk` of the decoder part, 256 threads): the `grid`
+// per-CTA gradient partials of the tile kernel split over 8 warps and combined in a fixed
+// order (deterministic).  CTA 0 also reduces the loss partials into loss_out[step].
+__device__ __forceinline__ void decoder_block(const Model& M, const StepRec& s, int blk,
+                                              const float* __restrict__ dW_partial,
+                                              const double* __restrict__ loss_partial, int grid,
+                                              double* __restrict__ loss_out)
+{
+  __shared__ float red[kDecWarps][32];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  if (blk == 0 && wp == 0) {
+    double l = 0.0;
+    for (int i = lane; i < grid; i += 32) l += loss_partial[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if (lane == 0 && loss_out) loss_out[s.step] = l / ((double)M.C * (double)s.texels);
+  }
+  // upstream updates all of W0, W1 and the first C rows of Wout (libopenntc.cpp:722-754)
+  const int nupd = min(M.nW, wo_off(M.F) + M.C * kHidden);
+  const int w = blk * 32 + lane;
+  float g = 0.0f;
+  if (w < nupd) {
+#pragma unroll 4
+    for (int i = wp; i < grid; i += kDecWarps) g += dW_partial[(size_t)i * M.nW + w];
+  }
+  red[wp][lane] = g;
+  __syncthreads();
+  if (wp != 0 || w >= nupd) return;
+  g = red[0][lane];
+#pragma unroll
+  for (int k = 1; k < kDecWarps; k++) g += red[k][lane];
+  float p = M.W[w], m = M.Wm[w], v = M.Wv[w];
+  adam1(p, m, v, g, s.lr_dec, s.b1, s.b2);
+  M.W[w] = p;
+  M.Wm[w] = m;
+  M.Wv[w] = v;
+}
+
+// ---- deferred latent optimiser ------------------------------------------------------------
+// Dense Adam touches every latent of the level every step.  Here a latent cell remembers how
+// many level steps it has received: max(applied[cell], floor), where the floor is the level
+// step up to which the whole level was last swept.  The steps a cell missed carry zero
+// gradient, so they are replayed from the ring of per-step (lr, bias1, bias2) exactly as the
+// dense update would have applied them (same adam1 arithmetic, same clamp), only later: right
+// before the cell is read again (catch-up over the step's footprint) or in a level sweep.
+
+// The C latents of one cell (contiguous, 8- or 16-byte aligned: C is even, buffers 256-byte).
+template <int C>
+__device__ __forceinline__ void load_cell(const float* __restrict__ src, int64_t e, float (&x)[C])
+{
+  if constexpr (C % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < C / 4; k++) {
+      const float4 t = reinterpret_cast<const float4*>(src + e)[k];
+      x[4 * k] = t.x, x[4 * k + 1] = t.y, x[4 * k + 2] = t.z, x[4 * k + 3] = t.w;
+    }
+  } else {
+    static_assert(C % 2 == 0, "latent channel counts are even");
+#pragma unroll
+    for (int k = 0; k < C / 2; k++) {
+      const float2 t = reinterpret_cast<const float2*>(src + e)[k];
+      x[2 * k] = t.x, x[2 * k + 1] = t.y;
+    }
+  }
+}
+
+template <int C>
+__device__ __forceinline__ void store_cell(float* __restrict__ dst, int64_t e, const float (&x)[C])
+{
+  if constexpr (C % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < C / 4; k++)
+      reinterpret_cast<float4*>(dst + e)[k] = make_float4(x[4 * k], x[4 * k + 1], x[4 * k + 2], x[4 * k + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < C / 2; k++) reinterpret_cast<float2*>(dst + e)[k] = make_float2(x[2 * k], x[2 * k + 1]);
+  }
+}
+
+// Replays level steps [a, J) with zero gradient on every channel of `cell`; the C channel
+// chains are independent, so they interleave.
+template <int C>
+__device__ __forceinline__ void replay_cell(const Pyramid& P, int lvl, int cell, int a, int J,
+                                            const float4* __restrict__ hist)
+{
+  const int64_t e = (int64_t)cell * C;
+  float p[C], m[C], v[C];
+  load_cell<C>(P.p[lvl], e, p);
+  load_cell<C>(P.m[lvl], e, m);
+  load_cell<C>(P.v[lvl], e, v);
+  for (int t = a; t < J; t++) {
+    const float4 h = hist[t & (kHistRing - 1)];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      adam1(p[c], m[c], v[c], 0.0f, h.x, h.y, h.z);
+      p[c] = clamp_latent(p[c], P.delta);
+    }
+  }
+  store_cell<C>(P.p[lvl], e, p);
+  store_cell<C>(P.m[lvl], e, m);
+  store_cell<C>(P.v[lvl], e, v);
+}
+
+// Applies the step's gradient to every channel of `cell` and clears it.
+template <int C>
+__device__ __forceinline__ void update_cell(const Pyramid& P, int lvl, int cell, float lr, float b1, float b2)
+{
+  const int64_t e = (int64_t)cell * C;
+  float p[C], m[C], v[C], g[C];
+  load_cell<C>(P.p[lvl], e, p);
+  load_cell<C>(P.m[lvl], e, m);
+  load_cell<C>(P.v[lvl], e, v);
+  load_cell<C>(P.g[lvl], e, g);
+#pragma unroll
+  for (int c = 0; c < C; c++) {
+    adam1(p[c], m[c], v[c], g[c], lr, b1, b2);
+    p[c] = clamp_latent(p[c], P.delta);
+    g[c] = 0.0f;
+  }
+  store_cell<C>(P.p[lvl], e, p);
+  store_cell<C>(P.m[lvl], e, m);
+  store_cell<C>(P.v[lvl], e, v);
+  store_cell<C>(P.g[lvl], e, g);
+}
+
+// Footprint cell `i` of F -> pyramid g and cell index in the level.
+__device__ __forceinline__ bool foot_cell(const FootRec& F, int i, const Model& M, int lvl, int& g, int& cell)
+{
+  g = i < F.cells[0] ? 0 : 1;
+  const int local = g ? i - F.cells[0] : i;
+  if (g == 1 && local >= F.cells[1]) return false;
+  int r = 0;
+  for (int k = 1; k < F.n[g]; k++) r = F.start[g][k] <= local ? k : r;
+  const int w = F.r[g][r][2];
+  const int q = local - F.start[g][r];
+  const int row = q / w;
+  const int dim = g == 0 ? M.g0.dim[lvl] : M.g1.dim[lvl];
+  cell = (F.r[g][r][1] + row) * dim + F.r[g][r][0] + (q - row * w);
+  return true;
+}
+
+template <int C0, int C1>
+__global__ void __launch_bounds__(256) catchup_kernel(Model M, const StepRec* __restrict__ steps, int idx,
+                                                      const __grid_constant__ FootRec F)
+{
+  const StepRec& s = steps[idx];
+  const int lvl = s.level, j = s.gstep, fl = s.gfloor;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int g, cell;
+  if (!foot_cell(F, i, M, lvl, g, cell)) return;
+  const int a = max(M.applied[g][lvl][cell], fl);
+  if (a >= j) return;
+  if (g == 0)
+    replay_cell<C0>(M.g0, lvl, cell, a, j, M.hist[lvl]);
+  else
+    replay_cell<C1>(M.g1, lvl, cell, a, j, M.hist[lvl]);
+}
+
+// Brings every cell of level `lvl` from max(applied, fl) up to J.  Writes no counter: the
+// caller raises the level's floor to J.
+template <int C0, int C1>
+__global__ void __launch_bounds__(256) sweep_kernel(Model M, int lvl, int fl, int J)
+{
+  const int n0 = M.g0.dim[lvl] * M.g0.dim[lvl];
+  const int n1 = M.g1.dim[lvl] * M.g1.dim[lvl];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0 + n1; i += gridDim.x * blockDim.x) {
+    const int g = i < n0 ? 0 : 1;
+    const int cell = g ? i - n0 : i;
+    const int a = max(M.applied[g][lvl][cell], fl);
+    if (a >= J) continue;
+    if (g == 0)
+      replay_cell<C0>(M.g0, lvl, cell, a, J, M.hist[lvl]);
+    else
+      replay_cell<C1>(M.g1, lvl, cell, a, J, M.hist[lvl]);
+  }
+}
+
+// Decoder Adam (CTAs [0, n_dec)) and the step's gradient on its footprint, every cell of which
+// is at level step gstep (the other CTAs).
+template <int C0, int C1>
+__global__ void __launch_bounds__(256) footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx,
+                                                               const __grid_constant__ FootRec F,
+                                                               const float* __restrict__ dW_partial,
+                                                               const double* __restrict__ loss_partial, int grid,
+                                                               double* __restrict__ loss_out, int n_dec)
+{
+  const StepRec& s = steps[idx];
+  if ((int)blockIdx.x < n_dec) {
+    decoder_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
+    return;
+  }
+  const int lvl = s.level, j = s.gstep;
+  const int i = (blockIdx.x - n_dec) * blockDim.x + threadIdx.x;
+  if (i == 0) M.hist[lvl][j & (kHistRing - 1)] = make_float4(s.lr_grid, s.gb1, s.gb2, 0.0f);
+  int g, cell;
+  if (!foot_cell(F, i, M, lvl, g, cell)) return;
+  if (g == 0)
+    update_cell<C0>(M.g0, lvl, cell, s.lr_grid, s.gb1, s.gb2);
+  else
+    update_cell<C1>(M.g1, lvl, cell, s.lr_grid, s.gb1, s.gb2);
+  M.applied[g][lvl][cell] = j + 1;
+}
+
 __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* __restrict__ steps, int step_idx,
                                                         const float* __restrict__ dW_partial,
                                                         const double* __restrict__ loss_partial, int grid,
@@ -64,30 +271,18 @@ __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* 
 {
   const StepRec& s = steps[step_idx];
   if ((int)blockIdx.x < n_dec_blocks) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w == 0 && loss_out) {
-      double l = 0.0;
-      for (int i = 0; i < grid; i++) l += loss_partial[i];
-      loss_out[s.step] = l / ((double)M.C * (double)s.texels);
-    }
-    // upstream updates all of W0, W1 and the first C rows of Wout (libopenntc.cpp:722-754)
-    if (w >= M.nW || w >= wo_off(M.F) + M.C * kHidden) return;
-    float g = 0.0f;
-    for (int i = 0; i < grid; i++) g += dW_partial[(size_t)i * M.nW + w];
-    float p = M.W[w], m = M.Wm[w], v = M.Wv[w];
-    adam1(p, m, v, g, s.lr_dec, s.b1, s.b2);
-    M.W[w] = p;
-    M.Wm[w] = m;
-    M.Wv[w] = v;
+    decoder_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
     return;
   }
   if (!s.grid_update) return;
   const int lvl = s.level;
+  const int b = blockIdx.x - n_dec_blocks;
+  const int nb = gridDim.x - n_dec_blocks;
   const long long n0 = (long long)M.g0.dim[lvl] * M.g0.dim[lvl] * M.g0.channels;
   const long long n1 = (long long)M.g1.dim[lvl] * M.g1.dim[lvl] * M.g1.channels;
   const long long q0 = n0 >> 2, q = q0 + (n1 >> 2);
-  const long long stride = (long long)(gridDim.x - n_dec_blocks) * blockDim.x;
-  for (long long i = (long long)(blockIdx.x - n_dec_blocks) * blockDim.x + threadIdx.x; i < q; i += stride) {
+  const long long stride = (long long)nb * blockDim.x;
+  for (long long i = (long long)b * blockDim.x + threadIdx.x; i < q; i += stride) {
     if (i < q0)
       adam_latent4(M.g0.p[lvl], M.g0.m[lvl], M.g0.v[lvl], M.g0.g[lvl], i << 2, s.lr_grid, s.gb1, s.gb2, M.g0.delta);
     else
@@ -141,20 +336,87 @@ __global__ void sum_doubles_kernel(const double* in, int n, double* out)
 
 }  // namespace
 
+static int sm_count()
+{
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+static int dec_blocks(const Model& M) { return (M.nW + 31) / 32; }
+
+// Profile channel pairs (C0, C1) with compiled deferred-optimiser kernels.
+#define ONTC_FOR_CHANNEL_PAIRS(X) X(8, 12) X(12, 20) X(12, 10) X(16, 12)
+
+cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+                           cudaStream_t stream)
+{
+  const int total = F.cells[0] + F.cells[1];
+  if (total <= 0) return cudaSuccess;
+#define X(a, b)                                                                          \
+  if (M.g0.channels == a && M.g1.channels == b) {                                        \
+    catchup_kernel<a, b><<<(total + 255) / 256, 256, 0, stream>>>(M, d_steps, step_idx, F); \
+    return cudaGetLastError();                                                           \
+  }
+  ONTC_FOR_CHANNEL_PAIRS(X)
+#undef X
+  return cudaErrorNotSupported;
+}
+
+cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+                                    const float* dW_partial, const double* loss_partial, int grid,
+                                    double* loss_out, cudaStream_t stream)
+{
+  const int total = std::max(1, F.cells[0] + F.cells[1]);
+  const int n_dec = dec_blocks(M);
+  const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);
+#define X(a, b)                                                                                          \
+  if (M.g0.channels == a && M.g1.channels == b) {                                                        \
+    footprint_update_kernel<a, b><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, loss_partial, \
+                                                              grid, loss_out, n_dec);                    \
+    return cudaGetLastError();                                                                           \
+  }
+  ONTC_FOR_CHANNEL_PAIRS(X)
+#undef X
+  return cudaErrorNotSupported;
+}
+
+cudaError_t launch_sweep(const Model& M, int level, int from, int J, cudaStream_t stream)
+{
+  const long long n = (long long)M.g0.dim[level] * M.g0.dim[level] + (long long)M.g1.dim[level] * M.g1.dim[level];
+  long long blocks = (n + 255) / 256;
+  if (blocks > (long long)sm_count() * 8) blocks = (long long)sm_count() * 8;
+#define X(a, b)                                                                          \
+  if (M.g0.channels == a && M.g1.channels == b) {                                        \
+    sweep_kernel<a, b><<<(unsigned)blocks, 256, 0, stream>>>(M, level, from, J);         \
+    return cudaGetLastError();                                                           \
+  }
+  ONTC_FOR_CHANNEL_PAIRS(X)
+#undef X
+  return cudaErrorNotSupported;
+}
+
+bool deferred_supported(int c0, int c1)
+{
+#define X(a, b) \
+  if (c0 == a && c1 == b) return true;
+  ONTC_FOR_CHANNEL_PAIRS(X)
+#undef X
+  return false;
+}
+
 cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, const float* dW_partial,
                              const double* loss_partial, int grid, double* loss_out, cudaStream_t stream)
 {
   // Sized for the largest level so one launch shape serves every step; CTAs beyond the
   // step level's work exit at once.
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int n_dec = (M.nW + 255) / 256;
+  const int n_dec = dec_blocks(M);
   const long long n0 = (long long)M.g0.dim[0] * M.g0.dim[0] * M.g0.channels;
   const long long n1 = (long long)M.g1.dim[0] * M.g1.dim[0] * M.g1.channels;
   long long quads = (n0 + n1) / 4;
   long long lat_blocks = (quads + 255) / 256;
-  if (lat_blocks > (long long)sms * 8) lat_blocks = (long long)sms * 8;
+  if (lat_blocks > (long long)sm_count() * 8) lat_blocks = (long long)sm_count() * 8;
   adam_step_kernel<<<(unsigned)(n_dec + lat_blocks), 256, 0, stream>>>(M, d_steps, step_idx, dW_partial, loss_partial,
                                                                         grid, loss_out, n_dec);
   return cudaGetLastError();

@@ -93,3 +93,29 @@ def test_product_path_refuses_to_run_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(openntc_b200, "LIB_PATH", tmp_path / "missing.so")
     with pytest.raises(RuntimeError):
         openntc_b200.load()
+
+
+def test_disjoint_cover_keeps_the_union(lib):
+    """The deferred optimiser's footprint cover: disjoint rectangles, same union as the input."""
+    import numpy as np
+    rng = np.random.default_rng(7)
+    for case in range(300):
+        n = int(rng.integers(0, 17))
+        dim = 64
+        x0 = rng.integers(0, dim, n); y0 = rng.integers(0, dim, n)
+        x1 = np.minimum(dim, x0 + rng.integers(1, 40, n)); y1 = np.minimum(dim, y0 + rng.integers(1, 40, n))
+        inp = np.stack([x0, y0, x1, y1], 1).astype(np.int32).copy()
+        out = np.zeros((256, 4), np.int32)
+        m = lib.ontc_debug_disjoint_cover(inp.ctypes.data, n, out.ctypes.data, 256)
+        assert m >= 0
+        want = np.zeros((dim, dim), np.int32)
+        for a, b, c, d in inp:
+            want[b:d, a:c] = 1
+        got = np.zeros((dim, dim), np.int32)
+        for a, b, c, d in out[:m]:
+            assert a < c and b < d
+            got[b:d, a:c] += 1
+        assert np.array_equal(got, want), case  # covered exactly once where the union is
+    one = np.array([[0, 0, 8, 8], [4, 4, 12, 12], [20, 0, 24, 4]], np.int32)
+    out = np.zeros((4, 4), np.int32)
+    assert lib.ontc_debug_disjoint_cover(one.ctypes.data, 3, out.ctypes.data, 2) == -1

@@ -1,0 +1,59 @@
+"""The deferred latent optimiser against the dense one.
+
+Upstream applies Adam to every latent of the step's level every step (libopenntc.cpp:755-790).
+The deferred optimiser updates only the footprint of the step and replays the zero-gradient
+steps a cell missed before it is read again.  Latent gradients are scattered with float
+atomics, so two training runs differ in the last bits whatever the optimiser; the comparison
+is therefore against the run-to-run spread of the dense optimiser itself."""
+import numpy as np
+import pytest
+
+import openntc_b200 as ont
+from openntc_b200 import _abi
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+GRADS = ((_abi.DBG_G0_GRAD, "g0"), (_abi.DBG_G1_GRAD, "g1"))
+
+
+def test_no_gradient_left_outside_footprints(materials):
+    """Every latent that received a gradient was inside its step's footprint: the deferred
+    update consumed (zeroed) all of them.  Four wrapped tiles per step on a 2048^2 chain."""
+    ctx = H.new_context(ont.Profile.Bpp_1_0, materials(2048, 5, 9), min_dim=16, grids=4, steps=400,
+                        precision=ont.Precision.BF16)
+    ctx.train(200)
+    sh = H.shape(ctx)
+    for l in range(sh["levels"]):
+        for which, name in GRADS:
+            g = H.tensor(ctx, which, l)
+            assert not g.any(), (name, l, int(np.count_nonzero(g)))
+
+
+def _run(manifest, mode, precision, steps):
+    ctx = H.new_context(ont.Profile.Bpp_0_5, manifest, min_dim=1024, grids=1, steps=steps, precision=precision,
+                        latent_adam=mode)
+    p = ctx.train_until_complete()
+    assert p.phase == ont.TrainPhase.TrainComplete and p.result == 0
+    sh = H.shape(ctx)
+    lat = {(k, l): H.tensor(ctx, k, l) for l in range(sh["levels"])
+           for k in (_abi.DBG_G0_M, _abi.DBG_G0_V, _abi.DBG_G1_M, _abi.DBG_G1_V)}
+    return ctx.eval().psnr, lat, ctx
+
+
+@pytest.mark.parametrize("precision", [ont.Precision.FP32, ont.Precision.BF16])
+def test_deferred_matches_dense(materials, precision):
+    """150 single-level steps (two ring sweeps, the lock flush, completion): PSNR and Adam
+    moments of the deferred run sit within the dense optimiser's own run-to-run spread."""
+    manifest = materials(1024, 6, 9)
+    psnr_a, a, ca = _run(manifest, ont.LatentAdam.DENSE, precision, 150)
+    psnr_b, b, cb = _run(manifest, ont.LatentAdam.DENSE, precision, 150)
+    psnr_d, d, cd = _run(manifest, ont.LatentAdam.DEFERRED, precision, 150)
+    print(f"PSNR dense {psnr_a:.4f} / {psnr_b:.4f}, deferred {psnr_d:.4f} dB")
+    assert abs(psnr_d - psnr_a) < max(4 * abs(psnr_b - psnr_a), 0.02)
+    for key in a:
+        spread = np.abs(b[key] - a[key]).max()
+        diff = np.abs(d[key] - a[key]).max()
+        scale = np.abs(a[key]).max()
+        assert diff <= max(4 * spread, 1e-3 * scale), (key, diff, spread, scale)
+    del ca, cb, cd
