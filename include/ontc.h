@@ -267,6 +267,21 @@ int ontc_kernel_times(ontc_context* ctx, ontc_kernel_time* out, int32_t max_clas
 /* Version string of the build ("ontc <git-describe> sm_100a"). */
 const char* ontc_version(void);
 
+/* ---- Mip reduction without device allocation (no upstream counterpart) -------------------
+ * One Lanczos-3 2x reduction (the arithmetic of ontc_debug_lanczos_down, upstream's
+ * filter_lanczos) of a DEVICE image d_src [dim][dim][ch] u8 into d_dst [dim/2][dim/2][ch],
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) without allocating
+ * device memory: for callers whose device memory belongs to their own pool, or that must not
+ * stall other streams (cudaFree synchronises the device).  The fp32 intermediate,
+ * dim * (dim/2) * ch floats, lives in one fixed device array per device; larger images
+ * return ONTC_INVALID_DIMENSION without touching the device (limit: 1024^2 x 4 channels,
+ * 2048^2 x 1).  ch 1..4.  Calls whose executions overlap (different streams, or host threads
+ * without ordering) race on that array: issue them on one stream or order them.  The first
+ * call on each device looks the array up (cudaGetSymbolAddress); make it before any stream
+ * capture on that device.  Returns when the work is enqueued. */
+#define ONTC_NOALLOC_SCRATCH_FLOATS 2097152
+int ontc_lanczos_down_noalloc(const uint8_t* d_src, int32_t dim, int32_t ch, uint8_t* d_dst, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

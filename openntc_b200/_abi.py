@@ -148,6 +148,7 @@ SIGNATURES = {
     "ontc_debug_package": (C.c_int, [P, C.c_int32, C.c_void_p]),
     "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
     "ontc_debug_disjoint_cover": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "ontc_lanczos_down_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
 }
 
 
