@@ -1,8 +1,8 @@
 // BF16 tensor-core tile kernel for one training step (sm_100a, tcgen05 + TMEM).
 //
-// A CTA (one per SM, persistent) runs two independent 4-warp groups.  Each group owns one
-// 128-texel work unit at a time (thread = texel row = TMEM lane) and takes it through the
-// whole per-texel pipeline of upstream's step:
+// A CTA (one per SM, persistent) runs two independent 8-warp groups.  Each group owns one
+// 128-texel work unit at a time (two threads per texel row = TMEM lane, each taking half of
+// the row's columns) and takes it through the whole per-texel pipeline of upstream's step:
 //
 //   gather (ntc_kernel.cu:75-177)             -> X    [128 x Kp]  bf16, shared memory
 //   H0 = X  W0^T          (M128 N64  K=Kp)    -> TMEM, epilogue: A0 = hg(H0)
@@ -34,8 +34,8 @@ namespace ontc {
 
 namespace {
 
-constexpr int kThreads = 256;      // 2 groups x 128
-constexpr int kGroupThreads = 128;
+constexpr int kThreads = 512;      // 2 groups x 256
+constexpr int kGroupThreads = 256; // 2 threads per texel row: half 0 / half 1 of the columns
 constexpr uint32_t kTmemCols = 512;
 // TMEM column map: per group a 128-column window [128 g, 128 g + 128) holding
 //   H0/H1/dA1/dA0 at +0 (64), Y at +64 (16), and later dX at +0 (<= 96);
@@ -43,7 +43,8 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColW0 = 256;   // dW0     (<= 96 columns)
 constexpr uint32_t kColW1 = 352;   // dW1     (64)
 constexpr uint32_t kColWo = 416;   // dWout^T (16)
-constexpr int kFootFloats = 6144;  // per group, 24 KB
+constexpr int kFootFloats = 6144;  // per group, 24 KB: two staging buffers
+constexpr int kFootBuf = kFootFloats / 2;
 constexpr int kMaxBoxW = 64;       // latent box limits of the owner-computes scatter
 constexpr int kMaxBoxH = 32;
 
@@ -74,7 +75,7 @@ struct GroupPtrs {
   uint8_t* P0;   // [128][64]  A0, later dH0
   uint8_t* P1;   // [128][64]  A1, later dH1
   uint8_t* dY;   // [128][16]
-  float* foot;   // [kFootFloats]
+  float* foot;   // [2][kFootBuf]: the current unit's latent boxes and the next one's
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
@@ -140,7 +141,7 @@ __device__ __forceinline__ bool unit_footprint(const Model& M, const StepRec& s,
   foot_span(xa, xa + 15, s.mip_dim, d1, f1.x0, f1.w);
   foot_span(ya, ya + 7, s.mip_dim, d1, f1.y0, f1.h);
   return f0.w <= kMaxBoxW && f0.h <= kMaxBoxH && f1.w <= kMaxBoxW && f1.h <= kMaxBoxH &&
-         f0.w * f0.h * SH::C0 + f1.w * f1.h * SH::C1 <= kFootFloats;
+         f0.w * f0.h * SH::C0 + f1.w * f1.h * SH::C1 <= kFootBuf;
 }
 
 // Which texel columns / rows of a unit touch each box column / row, per corner side: bit t
@@ -187,10 +188,12 @@ __device__ __forceinline__ void build_masks(const StepRec& s, int d0, int d1, co
   }
 }
 
-// Copies the unit's latent boxes (plus this step's noise) into shared memory.
+// Starts the asynchronous copy of a unit's latent boxes into a staging buffer.  Thread gt
+// copies elements gt, gt + 256, ...; add_noise then treats the same elements, so each thread
+// only needs its own copies complete.
 template <class SH>
-__device__ __forceinline__ void stage_footprint(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
-                                                float* foot, int gt)
+__device__ __forceinline__ void stage_copy(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
+                                           float* foot, int gt)
 {
   const int lvl = s.level;
   {
@@ -200,15 +203,7 @@ __device__ __forceinline__ void stage_footprint(const Model& M, const StepRec& s
     const float* p0 = M.g0.p[lvl];
     for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
       const int r = v / rowq, q = v - r * rowq;
-      const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
-      float4 val = *reinterpret_cast<const float4*>(p0 + e);
-      if (s.noise) {
-        val.x += latent_noise(M, s, 0u, (uint32_t)e);
-        val.y += latent_noise(M, s, 0u, (uint32_t)(e + 1));
-        val.z += latent_noise(M, s, 0u, (uint32_t)(e + 2));
-        val.w += latent_noise(M, s, 0u, (uint32_t)(e + 3));
-      }
-      *reinterpret_cast<float4*>(foot + r * f0.w * C0 + q * 4) = val;
+      ptx::cp_async16(foot + r * f0.w * C0 + q * 4, p0 + ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4);
     }
   }
   {
@@ -219,28 +214,66 @@ __device__ __forceinline__ void stage_footprint(const Model& M, const StepRec& s
     float* foot1 = foot + f0.w * f0.h * SH::C0;
     for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
       const int r = v / rowh, q = v - r * rowh;
-      const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
-      float2 val = *reinterpret_cast<const float2*>(p1 + e);
-      if (s.noise) {
-        val.x += latent_noise(M, s, 1u, (uint32_t)e);
-        val.y += latent_noise(M, s, 1u, (uint32_t)(e + 1));
-      }
-      *reinterpret_cast<float2*>(foot1 + r * f1.w * C1 + q * 2) = val;
+      ptx::cp_async8(foot1 + r * f1.w * C1 + q * 2, p1 + ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2);
     }
   }
 }
 
-// Gathers one texel's feature row (draw_features arithmetic).  `staged` reads the latents
-// (noise already added) from the shared-memory boxes, otherwise from global memory.
+// Adds this step's quantisation noise to the staged latents this thread copied.
 template <class SH>
-__device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, int x, int y, bool valid, int row,
-                                          bool staged, const Foot& f0, const Foot& f1, const float* foot, uint8_t* sX)
+__device__ __forceinline__ void stage_noise(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
+                                            float* foot, int gt)
+{
+  const int lvl = s.level;
+  {
+    constexpr int C0 = SH::C0;
+    const int d0 = M.g0.dim[lvl];
+    const int rowq = f0.w * (C0 / 4);
+    for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
+      const int r = v / rowq, q = v - r * rowq;
+      const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
+      float4* dst = reinterpret_cast<float4*>(foot + r * f0.w * C0 + q * 4);
+      float4 val = *dst;
+      val.x += latent_noise(M, s, 0u, (uint32_t)e);
+      val.y += latent_noise(M, s, 0u, (uint32_t)(e + 1));
+      val.z += latent_noise(M, s, 0u, (uint32_t)(e + 2));
+      val.w += latent_noise(M, s, 0u, (uint32_t)(e + 3));
+      *dst = val;
+    }
+  }
+  {
+    constexpr int C1 = SH::C1;
+    const int d1 = M.g1.dim[lvl];
+    const int rowh = f1.w * (C1 / 2);
+    float* foot1 = foot + f0.w * f0.h * SH::C0;
+    for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
+      const int r = v / rowh, q = v - r * rowh;
+      const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
+      float2* dst = reinterpret_cast<float2*>(foot1 + r * f1.w * C1 + q * 2);
+      float2 val = *dst;
+      val.x += latent_noise(M, s, 1u, (uint32_t)e);
+      val.y += latent_noise(M, s, 1u, (uint32_t)(e + 1));
+      *dst = val;
+    }
+  }
+}
+
+// Gathers half of one texel's feature row (draw_features arithmetic): half 0 the 4 C0 g0
+// corner features, half 1 the C1 bilinear g1 features, positional encoding, lod and padding.
+// `staged` reads the latents (noise already added) from the shared-memory boxes, otherwise
+// from global memory.
+template <class SH>
+__device__ __forceinline__ void gather_half(const Model& M, const StepRec& s, int x, int y, bool valid, int row,
+                                           int half, bool staged, const Foot& f0, const Foot& f1, const float* foot,
+                                           uint8_t* sX)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
+  constexpr int kSplit = 4 * C0;  // a multiple of 8: chunk-aligned
+  static_assert(kSplit % 8 == 0, "feature split must be chunk-aligned");
+  const int col0 = half ? kSplit : 0, col1 = half ? Kp : kSplit;
   if (!valid) {
     const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int c = 0; c < Kp; c += 8) st_chunk(sX, row, c, Kp, z);
+    for (int c = col0; c < col1; c += 8) st_chunk(sX, row, c, Kp, z);
     return;
   }
   const int lvl = s.level;
@@ -249,39 +282,42 @@ __device__ __forceinline__ void gather_row(const Model& M, const StepRec& s, int
   Gather G;
   gather_geometry(x, y, s.mip_dim, d0, d1, G);
   float buf[8];
-  int f = 0;
+  int f = 0;  // features put so far (compile-time after unrolling, so buf stays in registers)
   auto put = [&](float v) {
     buf[f & 7] = v;
     f++;
-    if ((f & 7) == 0) st_chunk(sX, row, f - 8, Kp, buf);
+    if ((f & 7) == 0) st_chunk(sX, row, col0 + f - 8, Kp, buf);
   };
+  if (half == 0) {
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    if (staged) {
-      const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
-      const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
+    for (int k = 0; k < 4; k++) {
+      if (staged) {
+        const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
+        const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
 #pragma unroll
-      for (int c = 0; c < C0; c += 4) {
-        const float4 q = *reinterpret_cast<const float4*>(src + c);
-        put(q.x);
-        put(q.y);
-        put(q.z);
-        put(q.w);
-      }
-    } else {
-      const int base = G.c0[k] * C0;
-      const float* p0 = M.g0.p[lvl];
+        for (int c = 0; c < C0; c += 4) {
+          const float4 q = *reinterpret_cast<const float4*>(src + c);
+          put(q.x);
+          put(q.y);
+          put(q.z);
+          put(q.w);
+        }
+      } else {
+        const int base = G.c0[k] * C0;
+        const float* p0 = M.g0.p[lvl];
 #pragma unroll
-      for (int c = 0; c < C0; c += 4) {
-        const float4 q = *reinterpret_cast<const float4*>(p0 + base + c);
-        float v[4] = {q.x, q.y, q.z, q.w};
+        for (int c = 0; c < C0; c += 4) {
+          const float4 q = *reinterpret_cast<const float4*>(p0 + base + c);
+          float v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          if (s.noise) v[i] = v[i] + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
-          put(v[i]);
+          for (int i = 0; i < 4; i++) {
+            if (s.noise) v[i] = v[i] + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
+            put(v[i]);
+          }
         }
       }
     }
+    return;
   }
   float acc[C1];
 #pragma unroll
@@ -377,6 +413,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp, F = SH::F;
   constexpr uint32_t SX = SH::SX;
+  constexpr int KH = Kp / 2;  // dX columns per half row (a multiple of 8)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t tmem_base_s;
@@ -385,11 +422,14 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   __shared__ float u8_to_unit[256];  // v / 255 as upstream computes it (libopenntc draw_targets)
   __shared__ CornerMasks masks_s[2];
 
-  const StepRec s = steps[step_idx];
+  const StepRec& s = steps[step_idx];  // read through L1: a register copy would not fit
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  const int g = tid >> 7;          // group
-  const int gt = tid & 127;        // thread within group == texel row == TMEM lane
+  const int g = tid >> 8;          // group
+  const int gt = tid & 255;        // thread within the group
+  const int row = gt & 127;        // texel row == TMEM lane
+  const int half = gt >> 7;        // which half of the row's columns this thread takes
+  const int part = g * 2 + half;   // 0..3: splits the per-CTA epilogue work
   const int quad = warp & 3;       // TMEM lane quadrant this warp may access
   const int C = M.C;
 
@@ -412,15 +452,16 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   }
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
   load_weights<SH>(M, sW0, sW1, sWo);
-  u8_to_unit[tid] = (float)tid / 255.0f;
+  if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
   ptx::fence_after_sync();
   const uint32_t tbase = tmem_base_s;
   const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
-  // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16)
-  for (uint32_t c = kColW0 + 16 * (uint32_t)g; c < kColWo + 16; c += 32) tmem_st_zero16(tbase + lane_off + c);
+  // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16): each of
+  // the 4 parts takes every 4th 16-column chunk of its quadrant's lanes
+  for (uint32_t c = kColW0 + 16 * (uint32_t)part; c < kColWo + 16; c += 64) tmem_st_zero16(tbase + lane_off + c);
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   ptx::fence_before_sync();
   __syncthreads();
@@ -462,18 +503,52 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   const uint32_t aX = ptx::smem_addr(gp.X), aP0 = ptx::smem_addr(gp.P0), aP1 = ptx::smem_addr(gp.P1);
   const uint32_t adY = ptx::smem_addr(gp.dY);
   const uint32_t aW0 = ptx::smem_addr(sW0), aW1 = ptx::smem_addr(sW1), aWo = ptx::smem_addr(sWo);
+  const int hc = half * 32;  // this thread's first column of a 64-column tile
 
-  for (int unit = blockIdx.x * 2 + g; unit < ntiles; unit += gridDim.x * 2) {
+  // latent boxes: unit k's were copied (asynchronously) while unit k-1 ran
+  const int ustride = gridDim.x * 2;
+  Foot nf0 = {}, nf1 = {};
+  bool nstaged = false;
+  int pb = 0;
+  {
+    const int u0 = blockIdx.x * 2 + g;
+    nstaged = u0 < ntiles && unit_footprint<SH>(M, s, u0, nf0, nf1);
+    if (nstaged) stage_copy<SH>(M, s, nf0, nf1, gp.foot, gt);
+    ptx::cp_async_commit();
+  }
+
+  for (int unit = blockIdx.x * 2 + g; unit < ntiles; unit += ustride) {
     // ------------------------------------------------------------------ gather
-    const int b = unit * kTile + gt;
+    const int b = unit * kTile + row;
     const bool valid = b < s.texels;
     int x = 0, y = 0;
     if (valid) texel_xy(s, b, x, y);
-    Foot f0, f1;
-    const bool staged = unit_footprint<SH>(M, s, unit, f0, f1);
+    // this thread's target channels [8 half, 8 half + 8), fetched now, used after layer 2
+    uint32_t tq[2] = {0u, 0u};
+    if (valid) {
+      const uint8_t* tp = target + ((size_t)y * s.mip_dim + x) * C;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int c = half * 8 + j;
+        if (c < C) tq[j >> 2] |= (uint32_t)tp[c] << (8 * (j & 3));
+      }
+    }
+    const Foot f0 = nf0, f1 = nf1;
+    const bool staged = nstaged;
+    float* foot = gp.foot + pb * kFootBuf;
+    {
+      // start the next unit's copy into the other buffer (its last reader, the gather of
+      // the unit before this one, finished several group barriers ago)
+      const int nu = unit + ustride;
+      nstaged = nu < ntiles && unit_footprint<SH>(M, s, nu, nf0, nf1);
+      if (nstaged) stage_copy<SH>(M, s, nf0, nf1, gp.foot + (pb ^ 1) * kFootBuf, gt);
+      ptx::cp_async_commit();
+      pb ^= 1;
+    }
     CornerMasks& cm = masks_s[g];
     if (staged) {
-      stage_footprint<SH>(M, s, f0, f1, gp.foot, gt);
+      ptx::cp_async_wait<1>();  // this unit's copies (all but the group just committed)
+      if (s.noise) stage_noise<SH>(M, s, f0, f1, foot, gt);
       for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) {
         uint32_t* m = i < 2 * kMaxBoxW ? &cm.xlo[0][0] + i
                       : i < 4 * kMaxBoxW ? &cm.xhi[0][0] + (i - 2 * kMaxBoxW)
@@ -484,7 +559,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       bar_group(g);
       build_masks(s, M.g0.dim[s.level], M.g1.dim[s.level], f0, f1, unit, cm, gt);
     }
-    gather_row<SH>(M, s, x, y, valid, gt, staged, f0, f1, gp.foot, gp.X);
+    gather_half<SH>(M, s, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -496,18 +571,16 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 0 epilogue
-    float h0[64], h1[64];
-    ptx::ld16(lwin + 0, h0);
-    ptx::ld16(lwin + 16, h0 + 16);
-    ptx::ld16(lwin + 32, h0 + 32);
-    ptx::ld16(lwin + 48, h0 + 48);
+    float h0[32], h1[32];
+    ptx::ld16(lwin + hc, h0);
+    ptx::ld16(lwin + hc + 16, h0 + 16);
     ptx::ld_wait();
 #pragma unroll
-    for (int c = 0; c < 64; c += 8) {
+    for (int c = 0; c < 32; c += 8) {
       float a[8];
 #pragma unroll
       for (int j = 0; j < 8; j++) a[j] = hg_fast(h0[c + j]);
-      st_chunk(gp.P0, gt, c, 64, a);
+      st_chunk(gp.P0, row, hc + c, 64, a);
     }
     handoff();
     if (issuer) {
@@ -520,17 +593,15 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 1 epilogue
-    ptx::ld16(lwin + 0, h1);
-    ptx::ld16(lwin + 16, h1 + 16);
-    ptx::ld16(lwin + 32, h1 + 32);
-    ptx::ld16(lwin + 48, h1 + 48);
+    ptx::ld16(lwin + hc, h1);
+    ptx::ld16(lwin + hc + 16, h1 + 16);
     ptx::ld_wait();
 #pragma unroll
-    for (int c = 0; c < 64; c += 8) {
+    for (int c = 0; c < 32; c += 8) {
       float a[8];
 #pragma unroll
       for (int j = 0; j < 8; j++) a[j] = hg_fast(h1[c + j]);
-      st_chunk(gp.P1, gt, c, 64, a);
+      st_chunk(gp.P1, row, hc + c, 64, a);
     }
     handoff();
     if (issuer) {
@@ -545,21 +616,20 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
     // ------------------------------------------------------------------ output, residual, dY
     {
-      float yv[16], d[16];
-      ptx::ld16(lwin + 64, yv);
+      float yv[8], d[8];
+      ptx::ld8(lwin + 64 + half * 8, yv);
       ptx::ld_wait();
-      const uint8_t* tp = target + ((size_t)y * s.mip_dim + x) * C;
 #pragma unroll
-      for (int c = 0; c < 16; c++) {
-        d[c] = 0.0f;
+      for (int j = 0; j < 8; j++) {
+        const int c = half * 8 + j;
+        d[j] = 0.0f;
         if (valid && c < C) {
-          const float r = u8_to_unit[tp[c]] - yv[c];
+          const float r = u8_to_unit[(tq[j >> 2] >> (8 * (j & 3))) & 255u] - yv[j];
           loss += (double)r * (double)r;
-          d[c] = inv * r;
+          d[j] = inv * r;
         }
       }
-      st_chunk(gp.dY, gt, 0, 16, d);
-      st_chunk(gp.dY, gt, 8, 16, d + 8);
+      st_chunk(gp.dY, row, half * 8, 16, d);
     }
     handoff();
     if (issuer) {
@@ -577,18 +647,16 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
     // ------------------------------------------------------------------ dH1 (into P1)
     {
-      float da[64];
-      ptx::ld16(lwin + 0, da);
-      ptx::ld16(lwin + 16, da + 16);
-      ptx::ld16(lwin + 32, da + 32);
-      ptx::ld16(lwin + 48, da + 48);
+      float da[32];
+      ptx::ld16(lwin + hc, da);
+      ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
 #pragma unroll
-      for (int c = 0; c < 64; c += 8) {
+      for (int c = 0; c < 32; c += 8) {
         float gv[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h1[c + j]);
-        st_chunk(gp.P1, gt, c, 64, gv);
+        st_chunk(gp.P1, row, hc + c, 64, gv);
       }
     }
     handoff();
@@ -610,18 +678,16 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
     // ------------------------------------------------------------------ dH0 (into P0)
     {
-      float da[64];
-      ptx::ld16(lwin + 0, da);
-      ptx::ld16(lwin + 16, da + 16);
-      ptx::ld16(lwin + 32, da + 32);
-      ptx::ld16(lwin + 48, da + 48);
+      float da[32];
+      ptx::ld16(lwin + hc, da);
+      ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
 #pragma unroll
-      for (int c = 0; c < 64; c += 8) {
+      for (int c = 0; c < 32; c += 8) {
         float gv[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h0[c + j]);
-        st_chunk(gp.P0, gt, c, 64, gv);
+        st_chunk(gp.P0, row, hc + c, 64, gv);
       }
     }
     handoff();
@@ -645,60 +711,58 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (s.grid_update) {
       const int lvl = s.level;
       const int d0 = M.g0.dim[lvl], d1 = M.g1.dim[lvl];
-      // all Kp feature-gradient columns, in 16-column aligned TMEM loads
-      float dx[Kp];
+      // dX rows to shared memory (the group's operand tiles are free now), half a row per thread
+      constexpr int LD = Kp + 4;
+      float* dxs = reinterpret_cast<float*>(gp.X);
+      {
+        float dx[KH];
 #pragma unroll
-      for (int c = 0; c < Kp; c += 16) ptx::ld16(lwin + c, dx + c);
-      ptx::ld_wait();
+        for (int c = 0; c < KH; c += 8) ptx::ld8(lwin + half * KH + c, dx + c);
+        ptx::ld_wait();
+#pragma unroll
+        for (int c = 0; c < KH; c += 4)
+          *reinterpret_cast<float4*>(dxs + row * LD + half * KH + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);
+      }
+      bar_group(g);
+      float* g0p = M.g0.g[lvl];
+      float* g1p = M.g1.g[lvl];
       if (staged) {
-        // owner-computes: dX rows to shared memory (the group's operand tiles are free now),
-        // then each thread sums the contributions to the latent elements it owns
-        constexpr int LD = Kp + 4;
-        float* dxs = reinterpret_cast<float*>(gp.X);
-#pragma unroll
-        for (int c = 0; c < Kp; c += 4)
-          *reinterpret_cast<float4*>(dxs + gt * LD + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);
-        bar_group(g);
-        // one thread per box cell sums all channels of that cell
+        // owner-computes: a work item is one box cell and a group of its channels (4 of g0,
+        // 2 of g1); its thread sums every texel-corner contribution to them
+        constexpr int Q0 = C0 / 4, Q1 = C1 / 2;
         const int nc0 = f0.w * f0.h;
-        const int nc = nc0 + f1.w * f1.h;
-        float* g0p = M.g0.g[lvl];
-        float* g1p = M.g1.g[lvl];
-        for (int i = gt; i < nc; i += kGroupThreads) {
-          if (i < nc0) {
-            const int by = i / f0.w, bx = i - by * f0.w;
-            float sum[C0];
-#pragma unroll
-            for (int c = 0; c < C0; c++) sum[c] = 0.0f;
+        const int ni0 = nc0 * Q0;
+        const int ni = ni0 + f1.w * f1.h * Q1;
+        for (int i = gt; i < ni; i += kGroupThreads) {
+          if (i < ni0) {
+            const int cell = i / Q0, q = i - cell * Q0;
+            const int by = cell / f0.w, bx = cell - by * f0.w;
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
               const uint32_t mx = (kk & 1) ? cm.xhi[0][bx] : cm.xlo[0][bx];
               const uint32_t my = (kk & 2) ? cm.yhi[0][by] : cm.ylo[0][by];
               for (uint32_t ym = my; ym; ym &= ym - 1) {
-                const int ty = __ffs(ym) - 1;
+                const float* srow = dxs + ((__ffs(ym) - 1) << 4) * LD + kk * C0 + 4 * q;
                 for (uint32_t xm = mx; xm; xm &= xm - 1) {
-                  const float* src = dxs + ((ty << 4) + __ffs(xm) - 1) * LD + kk * C0;
-#pragma unroll
-                  for (int c = 0; c < C0; c += 4) {
-                    const float4 v = *reinterpret_cast<const float4*>(src + c);
-                    sum[c] += v.x;
-                    sum[c + 1] += v.y;
-                    sum[c + 2] += v.z;
-                    sum[c + 3] += v.w;
-                  }
+                  const float4 v = *reinterpret_cast<const float4*>(srow + (__ffs(xm) - 1) * LD);
+                  sum.x += v.x;
+                  sum.y += v.y;
+                  sum.z += v.z;
+                  sum.w += v.w;
                 }
               }
             }
-            float* dst = g0p + ((f0.y0 + by) * d0 + f0.x0 + bx) * C0;
-#pragma unroll
-            for (int c = 0; c < C0; c++)
-              if (sum[c] != 0.0f) atomicAdd(dst + c, sum[c]);
+            float* dst = g0p + ((f0.y0 + by) * d0 + f0.x0 + bx) * C0 + 4 * q;
+            if (sum.x != 0.0f) atomicAdd(dst, sum.x);
+            if (sum.y != 0.0f) atomicAdd(dst + 1, sum.y);
+            if (sum.z != 0.0f) atomicAdd(dst + 2, sum.z);
+            if (sum.w != 0.0f) atomicAdd(dst + 3, sum.w);
           } else {
-            const int j = i - nc0;
-            const int by = j / f1.w, bx = j - by * f1.w;
-            float sum[C1];
-#pragma unroll
-            for (int c = 0; c < C1; c++) sum[c] = 0.0f;
+            const int j = i - ni0;
+            const int cell = j / Q1, q = j - cell * Q1;
+            const int by = cell / f1.w, bx = cell - by * f1.w;
+            float2 sum = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
               const uint32_t mx = (kk & 1) ? cm.xhi[1][bx] : cm.xlo[1][bx];
@@ -707,46 +771,47 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
                 const int ty = __ffs(ym) - 1;
                 const float fy = cm.fy[ty];
                 const float wy = (kk & 2) ? fy : (1.0f - fy);
+                const float* srow = dxs + (ty << 4) * LD + 4 * C0 + 2 * q;
                 for (uint32_t xm = mx; xm; xm &= xm - 1) {
                   const int tx = __ffs(xm) - 1;
                   const float fx = cm.fx[tx];
                   // the bilinear weight exactly as gather_geometry forms it
                   const float w = ((kk & 1) ? fx : (1.0f - fx)) * wy;
-                  const float* src = dxs + ((ty << 4) + tx) * LD + 4 * C0;
-#pragma unroll
-                  for (int c = 0; c < C1; c += 2) {
-                    const float2 v = *reinterpret_cast<const float2*>(src + c);
-                    sum[c] += w * v.x;
-                    sum[c + 1] += w * v.y;
-                  }
+                  const float2 v = *reinterpret_cast<const float2*>(srow + tx * LD);
+                  sum.x += w * v.x;
+                  sum.y += w * v.y;
                 }
               }
             }
-            float* dst = g1p + ((f1.y0 + by) * d1 + f1.x0 + bx) * C1;
-#pragma unroll
-            for (int c = 0; c < C1; c++)
-              if (sum[c] != 0.0f) atomicAdd(dst + c, sum[c]);
+            float* dst = g1p + ((f1.y0 + by) * d1 + f1.x0 + bx) * C1 + 2 * q;
+            if (sum.x != 0.0f) atomicAdd(dst, sum.x);
+            if (sum.y != 0.0f) atomicAdd(dst + 1, sum.y);
           }
         }
       } else if (valid) {
-        // direct per-texel scatter (wrapped blocks, tiny tiles, oversized boxes)
+        // direct per-texel scatter (wrapped blocks, tiny tiles, oversized boxes): half 0 the
+        // g0 corners, half 1 the bilinear g1 corners of the row
         Gather G;
         gather_geometry(x, y, s.mip_dim, d0, d1, G);
-        float* g0p = M.g0.g[lvl];
-        float* g1p = M.g1.g[lvl];
+        const float* dxr = dxs + row * LD;
+        if (half == 0) {
 #pragma unroll
-        for (int kk = 0; kk < 4; kk++)
+          for (int kk = 0; kk < 4; kk++)
 #pragma unroll
-          for (int c = 0; c < C0; c++) atomicAdd(&g0p[G.c0[kk] * C0 + c], dx[kk * C0 + c]);
+            for (int c = 0; c < C0; c++) atomicAdd(&g0p[G.c0[kk] * C0 + c], dxr[kk * C0 + c]);
+        } else {
 #pragma unroll
-        for (int kk = 0; kk < 4; kk++)
+          for (int kk = 0; kk < 4; kk++)
 #pragma unroll
-          for (int c = 0; c < C1; c++) atomicAdd(&g1p[G.c1[kk] * C1 + c], G.w1[kk] * dx[4 * C0 + c]);
+            for (int c = 0; c < C1; c++) atomicAdd(&g1p[G.c1[kk] * C1 + c], G.w1[kk] * dxr[4 * C0 + c]);
+        }
       }
     }
     ptx::fence_before_sync();
     bar_group(g);
   }
+
+  ptx::cp_async_wait<0>();  // no copy may still target shared memory at exit
 
   // ------------------------------------------------------------------ weight gradients out
   const double ls = block_sum_d_tc(loss, red);
@@ -757,7 +822,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     const int lane = tid & 31;
     const int h = quad * 16 + lane;  // M=64 accumulators: row = lane of the quadrant's first 16
     const uint32_t la = tbase + lane_off;
-    for (int c = g * 8; c < Kp; c += 16) {  // dW0 [64][F], 8-column steps split by group
+    for (int c = part * 8; c < Kp; c += 32) {  // dW0 [64][F], 8-column steps split by part
       float v[8];
       ptx::ld8(la + kColW0 + c, v);
       ptx::ld_wait();
@@ -766,14 +831,13 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
           if (c + j < F) dst[w0_off() + h * F + c + j] = v[j];
     }
     {
-      float v[32];  // dW1[i][h]: accumulator row i, columns h
-      ptx::ld16(la + kColW1 + g * 32, v);
-      ptx::ld16(la + kColW1 + g * 32 + 16, v + 16);
+      float v[16];  // dW1[i][h]: accumulator row i, columns h, 16 per part
+      ptx::ld16(la + kColW1 + part * 16, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 32; j++) dst[w1_off(F) + h * 64 + g * 32 + j] = v[j];
+        for (int j = 0; j < 16; j++) dst[w1_off(F) + h * 64 + part * 16 + j] = v[j];
     }
-    {
+    if (half == 0) {
       float v[8];  // dWout^T[h][c] -> dWout[c][h]
       ptx::ld8(la + kColWo + g * 8, v);
       ptx::ld_wait();
