@@ -421,8 +421,11 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   __shared__ double red[kThreads / 32];
   __shared__ float u8_to_unit[256];  // v / 255 as upstream computes it (libopenntc draw_targets)
   __shared__ CornerMasks masks_s[2];
+  __shared__ StepRec step_s;
 
-  const StepRec& s = steps[step_idx];  // read through L1: a register copy would not fit
+  // The step record lives in shared memory: every group barrier (a memory clobber) makes the
+  // compiler re-read the fields it uses, and there that costs a shared load, not an L1/L2 trip.
+  const StepRec& s = step_s;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int g = tid >> 8;          // group
@@ -453,6 +456,9 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
   load_weights<SH>(M, sW0, sW1, sWo);
   if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
+  static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
+  if (tid < (int)(sizeof(StepRec) / 4))
+    reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(steps + step_idx)[tid];
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
@@ -523,15 +529,16 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     const bool valid = b < s.texels;
     int x = 0, y = 0;
     if (valid) texel_xy(s, b, x, y);
-    // this thread's target channels [8 half, 8 half + 8), fetched now, used after layer 2
-    uint32_t tq[2] = {0u, 0u};
+    // this thread's target channels [8 half, 8 half + 8): the loads are issued now and their
+    // values first used after layer 2, so their latency hides behind the forward pass
+    uint32_t tb[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) tb[j] = 0u;
     if (valid) {
       const uint8_t* tp = target + ((size_t)y * s.mip_dim + x) * C;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const int c = half * 8 + j;
-        if (c < C) tq[j >> 2] |= (uint32_t)tp[c] << (8 * (j & 3));
-      }
+      for (int j = 0; j < 8; j++)
+        if (half * 8 + j < C) tb[j] = tp[half * 8 + j];
     }
     const Foot f0 = nf0, f1 = nf1;
     const bool staged = nstaged;
@@ -624,7 +631,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         const int c = half * 8 + j;
         d[j] = 0.0f;
         if (valid && c < C) {
-          const float r = u8_to_unit[(tq[j >> 2] >> (8 * (j & 3))) & 255u] - yv[j];
+          const float r = u8_to_unit[tb[j]] - yv[j];
           loss += (double)r * (double)r;
           d[j] = inv * r;
         }
