@@ -63,10 +63,7 @@ enum { ONTC_PRECISION_BF16 = 0, ONTC_PRECISION_FP32 = 1 };
 
 /* Decoder arithmetic for ontc_decode (upstream: HLSL only, ntc_decode.hlsli:605-623). */
 enum {
-  ONTC_DECODE_INT8 = 0, /* SampleMaterial semantics, integer-exact with the DP4A path */
-  ONTC_DECODE_FP32 = 1, /* float model, fp32 weights */
-  ONTC_DECODE_BF16 = 2, /* float model, bf16 weights and activations */
-  ONTC_DECODE_FP8 = 3   /* float model, e4m3 weights with per-layer scales */
+  ONTC_DECODE_INT8 = 0 /* SampleMaterial semantics, integer-exact with the DP4A path */
 };
 
 /* openntc::CalibrationData, openntc_runtime.h:61-67 */
@@ -240,6 +237,27 @@ int ontc_profile_from_string(const char* s, int32_t* out_profile);
 const char* ontc_semantic_to_string(int32_t semantic);
 int32_t ontc_semantic_from_name(const char* name);
 int32_t ontc_channel_count_for_semantic(int32_t semantic);
+
+/* ---- Decode: SampleMaterial over a batch (ntc_decode.hlsli:605-623) --------------------
+ * Upstream decodes in HLSL only (one sample per shader invocation, DP4A or cooperative
+ * vectors).  Here a decoder holds one compressed material on the device and evaluates batches
+ * of samples with upstream's integer arithmetic: packed latents -> int8 features -> int8 MLP
+ * with per-row weight scales and per-layer activation scales -> saturate to [0, 1]. */
+
+/* Uploads `data` (per-level packed pyramids, int8 decoder blob, NTCConstants from
+ * ontc_fill_constants) to the current device.  mode: ONTC_DECODE_INT8.  stream: the
+ * cudaStream_t decodes run on (NULL = legacy default stream).  The data may be freed after
+ * the call.  Returns ONTC_INVALID_FILE when the data does not match its profile's shapes. */
+int ontc_decoder_create(const ontc_compressed_data* data, int32_t mode, void* stream, ontc_decoder** out);
+void ontc_decoder_destroy(ontc_decoder* dec);
+/* Decodes n samples from DEVICE buffers: d_uv [n][2] f32, d_lod [n] i32 (clamped to the mip
+ * range as upstream does), into d_out [n][channel_count] f32.  Enqueued on the decoder's
+ * stream; returns once enqueued. */
+int ontc_decode(ontc_decoder* dec, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out);
+/* The same from HOST buffers: copies in, decodes, copies out, and returns when done. */
+int ontc_decode_host(ontc_decoder* dec, const float* uv, const int32_t* lod, int64_t n, float* out);
+/* Waits for the decoder's stream; ONTC_CUDA_FAILURE if a decode failed or timed out. */
+int ontc_decoder_status(ontc_decoder* dec);
 
 /* ---- Library facts and kernel timing (no upstream counterpart) ------------------------- */
 

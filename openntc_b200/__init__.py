@@ -219,6 +219,46 @@ def fill_constants(data: CompressedData) -> Constants:
     return c
 
 
+class Decoder:
+    """Batch SampleMaterial (ntc_decode.hlsli:605-623) of one compressed material on the GPU."""
+
+    def __init__(self, data: CompressedData, stream: int | None = None):
+        self._lib = load()
+        h = C.c_void_p()
+        r = self._lib.ontc_decoder_create(C.byref(data), _abi.DECODE_INT8, stream, C.byref(h))
+        if r != 0:
+            raise RuntimeError(f"ontc_decoder_create failed: {Result(r).name}")
+        self._h = h.value
+        self.channels = data.channel_count
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ontc_decoder_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def decode_host(self, uv, lod):
+        """uv: float32 [n, 2], lod: int32 [n] (numpy) -> float32 [n, channels]."""
+        import numpy as np
+        uv = np.ascontiguousarray(uv, np.float32)
+        lod = np.ascontiguousarray(lod, np.int32)
+        out = np.empty((len(lod), self.channels), np.float32)
+        r = self._lib.ontc_decode_host(self._h, uv.ctypes.data, lod.ctypes.data, len(lod), out.ctypes.data)
+        if r != 0:
+            raise RuntimeError(f"ontc_decode_host failed: {Result(r).name}")
+        return out
+
+    def decode(self, d_uv: int, d_lod: int, n: int, d_out: int) -> Result:
+        """Device pointers; enqueued on the decoder's stream."""
+        return Result(self._lib.ontc_decode(self._h, d_uv, d_lod, n, d_out))
+
+    def status(self) -> Result:
+        return Result(self._lib.ontc_decoder_status(self._h))
+
+
 def semantic_from_name(name: str) -> int:
     return load().ontc_semantic_from_name(name.encode())
 

@@ -22,7 +22,7 @@ BPP_0_2, BPP_0_5, BPP_1_0, BPP_2_25 = range(4)
 QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH, QUALITY_ULTRA = range(4)
 MANIFEST_LOADED, TRAIN_IN_PROGRESS, TRAIN_COMPLETE, TRAIN_ERROR = 0, 1, 2, -1
 PRECISION_BF16, PRECISION_FP32 = 0, 1
-DECODE_INT8, DECODE_FP32, DECODE_BF16, DECODE_FP8 = range(4)
+DECODE_INT8 = 0  # ONTC_DECODE_INT8: SampleMaterial integer semantics
 
 
 class Calibration(C.Structure):
@@ -149,6 +149,11 @@ SIGNATURES = {
     "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
     "ontc_debug_disjoint_cover": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
     "ontc_lanczos_down_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ontc_decoder_create": (C.c_int, [C.POINTER(CompressedData), C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ontc_decoder_destroy": (None, [P]),
+    "ontc_decode": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "ontc_decode_host": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "ontc_decoder_status": (C.c_int, [P]),
 }
 
 

@@ -1,0 +1,410 @@
+// Decode kernel: upstream's SampleMaterial (ntc_decode.hlsli:605-623) for a batch of
+// (uv, lod) samples, with the arithmetic of its DP4A inference path (:410-502).
+//
+// A CTA (one per SM, persistent) runs kGroups independent 4-warp groups; a group owns a tile
+// of 128 samples at a time (thread = sample = TMEM lane):
+//
+//   features (GetFeaturesPacked, :196-342)  -> X  [128 x Kp] int8, shared memory
+//   acc0 = X  W0^T   (M128 N64 K=Kp, tcgen05 kind::i8, s32 in TMEM)
+//   a0   = q8(hg(acc0 * s0) / s_a1)          -> A  [128 x 64] int8 (over X)
+//   acc1 = a0 W1^T   (M128 N64 K=64)
+//   a1   = q8(hg(acc1 * s1) / s_a2)          -> A
+//   acc2 = a1 Wout^T (M128 N16 K=64)
+//   out  = saturate(acc2 * so)               -> global [n][C] f32
+//
+// The int8 products and int32 sums are exact, so the tensor cores reproduce the DP4A dot
+// products bit for bit; every float operation of the epilogues is written with explicit
+// round-to-nearest intrinsics in upstream's order, so outputs are bit-identical to the
+// HLSL semantics (as restated by the CPU oracle).  Every wait is bounded and reports a
+// timeout through the error word.
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "tc_ptx.cuh"
+
+namespace ontc {
+
+namespace {
+
+constexpr int kGroups = 4;
+constexpr int kGroupThreads = 128;
+constexpr int kThreads = kGroups * kGroupThreads;
+constexpr int kHid = 64;
+constexpr int kOutRows = 16;  // upstream's padded output rows (OUTP)
+
+// Compile-time profile shape (ntc_decode.hlsli:60-86): channels, bits, first-level mips.
+template <int C0_, int C1_, int B0_, int B1_, int L0MIPS_>
+struct DShape {
+  static constexpr int C0 = C0_, C1 = C1_, B0 = B0_, B1 = B1_, L0MIPS = L0MIPS_;
+  static constexpr int Fp = ((4 * C0 + C1 + 13 + 15) / 16) * 16;  // the blob's W0 row stride
+  static constexpr int Kp = ((Fp + 31) / 32) * 32;                // K of the i8 MMA (32 per step)
+};
+
+struct DecodeSmem {
+  static constexpr size_t kTile = 128 * 96;  // per group: X, then a0, then a1 (largest Kp = 96)
+};
+
+__device__ __forceinline__ uint32_t group_bar_id(int g) { return 1u + (uint32_t)g; }
+__device__ __forceinline__ void bar_group(int g)
+{
+  asm volatile("bar.sync %0, %1;" ::"r"(group_bar_id(g)), "r"(kGroupThreads) : "memory");
+}
+
+// The BITS bits of packed cell `cell` (bits [cell * BITS, (cell + 1) * BITS) of the level
+// starting at word `word_off`) as a little-endian stream of 32-bit words.  A code never
+// spans two words, so code c is (s[c*B / 32] >> (c*B % 32)) & mask.
+template <int BITS>
+__device__ __forceinline__ void cell_stream(const uint32_t* __restrict__ buf, uint32_t words, uint32_t word_off,
+                                            uint32_t cell, uint32_t (&s)[(BITS + 31) / 32])
+{
+  constexpr int NW = (BITS + 31) / 32;
+  const uint64_t bitpos = (uint64_t)cell * (uint64_t)BITS;
+  const uint64_t w = (uint64_t)word_off + (bitpos >> 5);  // 64-bit: never wraps past the bound check
+  if constexpr (BITS % 32 == 0) {
+#pragma unroll
+    for (int j = 0; j < NW; j++) s[j] = w + j < words ? __ldg(buf + w + j) : 0u;
+  } else {
+    uint32_t raw[NW + 1];
+#pragma unroll
+    for (int j = 0; j <= NW; j++) raw[j] = w + j < words ? __ldg(buf + w + j) : 0u;
+    const uint32_t off = (uint32_t)bitpos & 31u;
+#pragma unroll
+    for (int j = 0; j < NW; j++) s[j] = __funnelshift_r(raw[j], raw[j + 1], off);
+  }
+}
+
+template <int B>
+__device__ __forceinline__ uint32_t code_of(const uint32_t* s, int c)
+{
+  return (s[(c * B) >> 5] >> ((c * B) & 31)) & ((1u << B) - 1u);
+}
+
+// ClampS8(round(f)) with HLSL round = nearest, ties to even.  Clamping first leaves the
+// result unchanged (rounding is monotonic and the bounds are integers) and keeps |f| < 2^22,
+// where adding 1.5 * 2^23 rounds to an integer in the low mantissa bits.
+__device__ __forceinline__ int q8(float f)
+{
+  f = fminf(fmaxf(f, -128.0f), 127.0f);
+  return __float_as_int(__fadd_rn(f, 12582912.0f)) - 0x4B400000;
+}
+
+// x / 3 correctly rounded: RN(x * RN(1/3)) corrected once with the exact remainder
+// (division by a constant known in advance; checked against IEEE division for every float
+// with |x| <= 1.5, the only range hardgelu divides in).
+__device__ __forceinline__ float div3(float x)
+{
+  const float y = 1.0f / 3.0f;
+  const float q = __fmul_rn(x, y);
+  const float r = __fmaf_rn(-q, 3.0f, x);
+  return __fmaf_rn(r, y, q);
+}
+
+// hardgelu4 (ntc_decode.hlsli:400-403): x < -1.5 ? 0 : x < 1.5 ? (x / 3) * (x + 1.5) : x
+__device__ __forceinline__ float hg_hlsl(float x)
+{
+  const float mid = __fmul_rn(div3(x), __fadd_rn(x, 1.5f));
+  return x < -1.5f ? 0.0f : (x < 1.5f ? mid : x);
+}
+
+__device__ __forceinline__ void put_byte(uint32_t* w, int f, int v)
+{
+  w[f >> 2] |= ((uint32_t)v & 0xFFu) << (8 * (f & 3));
+}
+
+// GetFeaturesPacked (ntc_decode.hlsli:196-342) for one sample -> Kp signed bytes in w[].
+template <class SH>
+__device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, int lod, uint32_t* w)
+{
+  constexpr int C0 = SH::C0, C1 = SH::C1, B0 = SH::B0, B1 = SH::B1;
+  const ontc_constants& k = A.k;
+#pragma unroll
+  for (int i = 0; i < SH::Kp / 4; i++) w[i] = 0u;
+  lod = clampi(lod, 0, k.mip_count - 1);
+  const int lvl = lod < SH::L0MIPS ? 0 : 1 + (lod - SH::L0MIPS) / 2;
+  const int d0 = k.g0_grid_dim[lvl], d1 = k.g1_grid_dim[lvl];
+  const uint32_t o0 = k.g0_offset[lvl] >> 2, o1 = k.g1_offset[lvl] >> 2;
+  // g0: the 4 nearest cells, codes re-centred to signed bytes
+  {
+    const int gx = (int)floorf(__fsub_rn(__fmul_rn(u, (float)d0), 0.5f));
+    const int gy = (int)floorf(__fsub_rn(__fmul_rn(v, (float)d0), 0.5f));
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int cx = clampi(gx + (q & 1), 0, d0 - 1), cy = clampi(gy + (q >> 1), 0, d0 - 1);
+      uint32_t st[(C0 * B0 + 31) / 32];
+      cell_stream<C0 * B0>(A.g0, A.g0_words, o0, (uint32_t)(cy * d0 + cx), st);
+#pragma unroll
+      for (int c = 0; c < C0; c++) {
+        const uint32_t code = code_of<B0>(st, c);
+        put_byte(w, q * C0 + c, (int)((code << (8 - B0)) ^ 0x80u));
+      }
+    }
+  }
+  // g1: bilinear blend of the dequantised codes, then *128 to a signed byte
+  {
+    const float g1x = __fsub_rn(__fmul_rn(u, (float)d1), 0.5f);
+    const float g1y = __fsub_rn(__fmul_rn(v, (float)d1), 0.5f);
+    const float flx = floorf(g1x), fly = floorf(g1y);
+    const int hx = (int)flx, hy = (int)fly;
+    const float fx = __fsub_rn(g1x, flx), fy = __fsub_rn(g1y, fly);
+    const float ofx = __fsub_rn(1.0f, fx), ofy = __fsub_rn(1.0f, fy);
+    const float mult[4] = {__fmul_rn(ofx, ofy), __fmul_rn(fx, ofy), __fmul_rn(ofx, fy), __fmul_rn(fx, fy)};
+    const float half = (float)(1u << (B1 - 1));
+    float blend[C1];
+#pragma unroll
+    for (int c = 0; c < C1; c++) blend[c] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int cx = clampi(hx + (q & 1), 0, d1 - 1), cy = clampi(hy + (q >> 1), 0, d1 - 1);
+      uint32_t st[(C1 * B1 + 31) / 32];
+      cell_stream<C1 * B1>(A.g1, A.g1_words, o1, (uint32_t)(cy * d1 + cx), st);
+#pragma unroll
+      for (int c = 0; c < C1; c++) {
+        const uint32_t code = code_of<B1>(st, c);
+        blend[c] = __fmaf_rn(mult[q], __fdiv_rn(__fsub_rn((float)code, half), half), blend[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C1; c++) put_byte(w, 4 * C0 + c, q8(__fmul_rn(blend[c], 128.0f)));
+  }
+  // 12 triangle waves of the texel coordinate at this lod, then the normalised lod
+  {
+    const float cdim = (float)(k.dim >> lod);
+    const float tcx = floorf(__fmul_rn(u, cdim)), tcy = floorf(__fmul_rn(v, cdim));
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const float P = (float)(8 >> p);
+          const float c = a == 0 ? tcx : tcy;
+          const float ph = h == 0 ? 0.0f : __fmul_rn(0.25f, P);
+          const float t = __fdiv_rn(__fadd_rn(__fadd_rn(c, 0.5f), ph), P);
+          const float pe = __fsub_rn(1.0f, __fmul_rn(4.0f, fabsf(__fsub_rn(__fsub_rn(t, floorf(t)), 0.5f))));
+          put_byte(w, 4 * C0 + C1 + p * 4 + a * 2 + h, q8(__fmul_rn(pe, 128.0f)));
+        }
+    const float nl = __fdiv_rn((float)lod, (float)(k.mip_count - 1));
+    put_byte(w, 4 * C0 + C1 + 12, q8(__fmul_rn(nl, 128.0f)));
+  }
+}
+
+// Stores 16 consecutive int8 values (columns c0..c0+15, c0 % 16 == 0) of row r.
+__device__ __forceinline__ void st16(uint8_t* base, int r, int c0, int cols, uint32_t a, uint32_t b, uint32_t c,
+                                     uint32_t d)
+{
+  *reinterpret_cast<uint4*>(base + ptx::cm_off8(r, c0, cols)) = make_uint4(a, b, c, d);
+}
+
+// 16 accumulator columns of this thread's row -> 16 requantised activations (4 words).
+__device__ __forceinline__ void requant16(uint32_t taddr, const float* __restrict__ scale, float rcp, uint32_t* out)
+{
+  float acc[16];
+  ptx::ld16(taddr, acc);
+  ptx::ld_wait();
+#pragma unroll
+  for (int i = 0; i < 4; i++) out[i] = 0u;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const float x = __fmul_rn((float)__float_as_int(acc[j]), scale[j]);
+    const int a = q8(__fmul_rn(hg_hlsl(x), rcp));
+    out[j >> 2] |= ((uint32_t)a & 0xFFu) << (8 * (j & 3));
+  }
+}
+
+template <class SH>
+__device__ void load_decoder(const uint8_t* __restrict__ blob, uint8_t* W0, uint8_t* W1, uint8_t* Wo, float* s0,
+                             float* s1, float* so)
+{
+  constexpr int Fp = SH::Fp, Kp = SH::Kp;
+  // W0 [64][Fp] row-major in the blob -> canonical [64][Kp], zero past Fp
+  for (int i = threadIdx.x; i < kHid * Kp; i += kThreads) {
+    const int r = i / Kp, c = i - r * Kp;
+    W0[ptx::cm_off8(r, c, Kp)] = c < Fp ? blob[r * Fp + c] : 0;
+  }
+  const uint8_t* b1 = blob + kHid * Fp;
+  for (int i = threadIdx.x; i < kHid * kHid; i += kThreads) W1[ptx::cm_off8(i >> 6, i & 63, kHid)] = b1[i];
+  const uint8_t* bo = b1 + kHid * kHid;
+  for (int i = threadIdx.x; i < kOutRows * kHid; i += kThreads) Wo[ptx::cm_off8(i >> 6, i & 63, kHid)] = bo[i];
+  const float* sc = reinterpret_cast<const float*>(bo + kOutRows * kHid);
+  for (int i = threadIdx.x; i < kHid; i += kThreads) {
+    s0[i] = sc[i];
+    s1[i] = sc[kHid + i];
+  }
+  for (int i = threadIdx.x; i < kOutRows; i += kThreads) so[i] = sc[2 * kHid + i];
+}
+
+template <class SH>
+__global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_constant__ DecodeArgs A)
+{
+  constexpr int Kp = SH::Kp;
+  constexpr uint32_t SX = (Kp / 16) * 128;  // 8-row group stride of a [*][Kp] int8 tile
+  constexpr uint32_t S64 = (kHid / 16) * 128;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bars[kGroups];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int fail_s;
+  __shared__ float s0[kHid], s1[kHid], so[kOutRows];
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int g = tid >> 7;
+  const int row = tid & 127;
+  const int quad = warp & 3;
+  uint8_t* X = smem_raw + (size_t)g * DecodeSmem::kTile;
+  uint8_t* sW0 = smem_raw + (size_t)kGroups * DecodeSmem::kTile;
+  uint8_t* sW1 = sW0 + kHid * Kp;
+  uint8_t* sWo = sW1 + kHid * kHid;
+
+  if (tid == 0) {
+    for (int i = 0; i < kGroups; i++) ptx::mbar_init(&bars[i], 1);
+    ptx::fence_mbar_init();
+    fail_s = 0;
+  }
+  if (warp == 0) ptx::tmem_alloc(&tmem_base_s, 64 * kGroups);
+  load_decoder<SH>(A.blob, sW0, sW1, sWo, s0, s1, so);
+  ptx::fence_proxy_async();
+  ptx::fence_before_sync();
+  __syncthreads();
+  ptx::fence_after_sync();
+  const uint32_t tbase = tmem_base_s;
+  const uint32_t win = tbase + 64u * (uint32_t)g;
+  const uint32_t lwin = win + ((uint32_t)(quad * 32) << 16);
+  uint64_t* bar = &bars[g];
+  uint32_t phase = 0;
+  const bool issuer = row == 0, poller = (row >> 5) == 0;
+  const int C = A.k.channel_count;
+  const float rcp1 = A.k.rcp_s_a1, rcp2 = A.k.rcp_s_a2;
+
+  constexpr uint32_t I_L01 = ptx::idesc_s8(128, kHid, false, false);
+  constexpr uint32_t I_L2 = ptx::idesc_s8(128, kOutRows, false, false);
+  const uint32_t aX = ptx::smem_addr(X), aW0 = ptx::smem_addr(sW0), aW1 = ptx::smem_addr(sW1),
+                 aWo = ptx::smem_addr(sWo);
+
+  auto wait_mma = [&]() -> bool {
+    if (poller && !ptx::mbar_wait(bar, phase)) atomicExch(&fail_s, 1);
+    phase ^= 1u;
+    bar_group(g);
+    ptx::fence_after_sync();
+    return *(volatile int*)&fail_s == 0;
+  };
+  auto handoff = [&]() {
+    ptx::fence_proxy_async();
+    ptx::fence_before_sync();
+    bar_group(g);
+  };
+
+  const int64_t ntiles = (A.n + 127) / 128;
+  for (int64_t t = (int64_t)blockIdx.x * kGroups + g; t < ntiles; t += (int64_t)gridDim.x * kGroups) {
+    const int64_t i = t * 128 + row;
+    const bool valid = i < A.n;
+    // ---------------------------------------------------------------- features -> X
+    {
+      uint32_t w[Kp / 4];
+      if (valid) {
+        const float2 uv = reinterpret_cast<const float2*>(A.uv)[i];
+        features<SH>(A, uv.x, uv.y, A.lod[i], w);
+      } else {
+#pragma unroll
+        for (int j = 0; j < Kp / 4; j++) w[j] = 0u;
+      }
+#pragma unroll
+      for (int c = 0; c < Kp; c += 16) st16(X, row, c, Kp, w[c / 4], w[c / 4 + 1], w[c / 4 + 2], w[c / 4 + 3]);
+    }
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < Kp / 32; k++)
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, k > 0);
+      ptx::commit(bar);
+    }
+    if (!wait_mma()) break;
+    // ---------------------------------------------------------------- a0 -> A (over X)
+#pragma unroll
+    for (int c = 0; c < kHid; c += 16) {
+      uint32_t q[4];
+      requant16(lwin + c, s0 + c, rcp1, q);
+      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
+    }
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < kHid / 32; k++)
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, k > 0);
+      ptx::commit(bar);
+    }
+    if (!wait_mma()) break;
+    // ---------------------------------------------------------------- a1 -> A
+#pragma unroll
+    for (int c = 0; c < kHid; c += 16) {
+      uint32_t q[4];
+      requant16(lwin + c, s1 + c, rcp2, q);
+      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
+    }
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < kHid / 32; k++)
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, k > 0);
+      ptx::commit(bar);
+    }
+    if (!wait_mma()) break;
+    // ---------------------------------------------------------------- outputs
+    {
+      float acc[16];
+      ptx::ld16(lwin, acc);
+      ptx::ld_wait();
+      if (valid) {
+        float* o = A.out + i * C;
+#pragma unroll
+        for (int c = 0; c < kOutRows; c++)
+          if (c < C) {
+            const float y = __fmul_rn((float)__float_as_int(acc[c]), so[c]);
+            o[c] = fminf(1.0f, fmaxf(0.0f, y));  // saturate
+          }
+      }
+    }
+    // the next tile's features overwrite X only after every thread has read its outputs
+    ptx::fence_before_sync();
+    bar_group(g);
+  }
+  if (*(volatile int*)&fail_s != 0 && tid == 0) atomicExch(A.err, 1);
+  ptx::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) ptx::tmem_dealloc(tbase, 64 * kGroups);
+}
+
+template <class SH>
+cudaError_t launch_decode_shape(const DecodeArgs& A, int grid, cudaStream_t stream)
+{
+  constexpr size_t smem = kGroups * DecodeSmem::kTile + kHid * SH::Kp + kHid * kHid + kOutRows * kHid + 1024;
+  static_assert(smem <= 227 * 1024, "shared memory budget");
+  cudaError_t e = cudaFuncSetAttribute(decode_kernel<SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  decode_kernel<SH><<<grid, kThreads, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_decode(int profile, const DecodeArgs& A, cudaStream_t stream)
+{
+  if (A.n <= 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long tiles = (A.n + 127) / 128;
+  const int grid = (int)std::min<long long>(sms, (tiles + kGroups - 1) / kGroups);
+  switch (profile) {  // ntc_decode.hlsli:60-86
+    case 0: return launch_decode_shape<DShape<8, 12, 2, 4, 4>>(A, grid, stream);
+    case 1: return launch_decode_shape<DShape<12, 20, 4, 4, 4>>(A, grid, stream);
+    case 2: return launch_decode_shape<DShape<12, 10, 2, 4, 3>>(A, grid, stream);
+    case 3: return launch_decode_shape<DShape<16, 12, 4, 4, 3>>(A, grid, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace ontc

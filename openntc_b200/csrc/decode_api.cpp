@@ -1,0 +1,194 @@
+// C ABI of the batch decoder (include/ontc.h, "Decode"): one compressed material held on the
+// device, decoded with upstream's SampleMaterial arithmetic (ntc_decode.hlsli:605-623) by
+// launch_decode (decode.cu).  Upstream has no batch decode API: its decode is HLSL only.
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+#include "ontc.h"
+
+struct ontc_decoder {
+  int profile = 0;
+  cudaStream_t stream = nullptr;
+  ontc_constants k = {};
+  uint32_t* g0 = nullptr;
+  uint32_t* g1 = nullptr;
+  uint32_t g0_words = 0, g1_words = 0;
+  uint8_t* blob = nullptr;
+  int* err = nullptr;
+  // staging for ontc_decode_host, grown on demand
+  float* uv = nullptr;
+  int32_t* lod = nullptr;
+  float* out = nullptr;
+  int64_t cap = 0;
+};
+
+namespace {
+
+// Per-profile packing (ntc_decode.hlsli:60-86): channels, bits and the decoder blob size
+// (W0 [64][Fp] | W1 [64][64] | Wout [16][64] int8, then 64 + 64 + 16 float scales).
+struct ProfileShape {
+  int c0, c1, b0, b1, level0_mips;
+};
+bool profile_shape(int p, ProfileShape& s)
+{
+  switch (p) {
+    case ONTC_BPP_0_2: s = {8, 12, 2, 4, 4}; return true;
+    case ONTC_BPP_0_5: s = {12, 20, 4, 4, 4}; return true;
+    case ONTC_BPP_1_0: s = {12, 10, 2, 4, 3}; return true;
+    case ONTC_BPP_2_25: s = {16, 12, 4, 4, 3}; return true;
+    default: return false;
+  }
+}
+size_t blob_bytes(const ProfileShape& s)
+{
+  const size_t Fp = ((4 * s.c0 + s.c1 + 13 + 15) / 16) * 16;
+  return 64 * Fp + 64 * 64 + 16 * 64 + 4 * (64 + 64 + 16);
+}
+
+void release(ontc_decoder* d)
+{
+  cudaFree(d->g0);
+  cudaFree(d->g1);
+  cudaFree(d->blob);
+  cudaFree(d->err);
+  cudaFree(d->uv);
+  cudaFree(d->lod);
+  cudaFree(d->out);
+}
+
+// One pyramid, its levels at their byte offsets, into a fresh device buffer.
+int upload_pyramid(uint32_t* const* levels, const size_t* sizes, const size_t* offsets, int count, size_t total,
+                   uint32_t** dst, uint32_t* words)
+{
+  if (total == 0 || total % 4 != 0 || total / 4 > 0xFFFFFFFFull) return ONTC_INVALID_FILE;
+  for (int l = 0; l < count; l++)
+    if (!levels[l] || offsets[l] % 4 != 0 || offsets[l] + sizes[l] > total) return ONTC_INVALID_FILE;
+  if (cudaMalloc(dst, total) != cudaSuccess) return ONTC_ALLOCATION_FAILURE;
+  if (cudaMemset(*dst, 0, total) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  for (int l = 0; l < count; l++)
+    if (cudaMemcpy(reinterpret_cast<uint8_t*>(*dst) + offsets[l], levels[l], sizes[l], cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return ONTC_CUDA_FAILURE;
+  *words = (uint32_t)(total / 4);
+  return ONTC_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ontc_decoder_create(const ontc_compressed_data* data, int32_t mode, void* stream, ontc_decoder** out)
+{
+  if (!out) return ONTC_INVALID_STATE;
+  *out = nullptr;
+  if (!data || mode != ONTC_DECODE_INT8) return ONTC_INVALID_STATE;
+  ProfileShape ps;
+  if (!profile_shape(data->profile, ps)) return ONTC_INVALID_FILE;
+  if (data->g0_channels != ps.c0 || data->g1_channels != ps.c1 || data->g0_bits_per_channel != ps.b0 ||
+      data->g1_bits_per_channel != ps.b1 || data->level_count < 1 || data->level_count > ONTC_MAX_LEVELS ||
+      data->channel_count < 1 || data->channel_count > ONTC_MAX_CHANNELS || data->mip_count < 1 ||
+      data->mip_count > ONTC_MAX_MIPS || !data->decoder || data->decoder_size < blob_bytes(ps))
+    return ONTC_INVALID_FILE;
+  // every lod the decoder can be asked for (clamped to the mip range) must have its feature
+  // level, with non-empty power-of-two grids (FeatureLevelForLod, ntc_decode.hlsli:127-133)
+  const int last = data->mip_count - 1;
+  const int top = last < ps.level0_mips ? 0 : 1 + (last - ps.level0_mips) / 2;
+  if (top >= data->level_count) return ONTC_INVALID_FILE;
+  for (int l = 0; l <= top; l++) {
+    const int a = data->g0_grid_dim[l], b = data->g1_grid_dim[l];
+    if (a < 1 || b < 1 || (a & (a - 1)) || (b & (b - 1))) return ONTC_INVALID_FILE;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  ontc_decoder* d = new ontc_decoder();
+  d->profile = data->profile;
+  d->stream = static_cast<cudaStream_t>(stream);
+  ontc_fill_constants(data, &d->k);
+  int r = upload_pyramid(data->g0, data->g0_size, data->g0_offset, data->level_count, data->g0_total_size, &d->g0,
+                         &d->g0_words);
+  if (r == ONTC_SUCCESS)
+    r = upload_pyramid(data->g1, data->g1_size, data->g1_offset, data->level_count, data->g1_total_size, &d->g1,
+                       &d->g1_words);
+  if (r == ONTC_SUCCESS) {
+    if (cudaMalloc(&d->blob, data->decoder_size) != cudaSuccess || cudaMalloc(&d->err, sizeof(int)) != cudaSuccess)
+      r = ONTC_ALLOCATION_FAILURE;
+    else if (cudaMemcpy(d->blob, data->decoder, data->decoder_size, cudaMemcpyHostToDevice) != cudaSuccess ||
+             cudaMemset(d->err, 0, sizeof(int)) != cudaSuccess)
+      r = ONTC_CUDA_FAILURE;
+  }
+  if (r != ONTC_SUCCESS) {
+    release(d);
+    delete d;
+    return r;
+  }
+  *out = d;
+  return ONTC_SUCCESS;
+}
+
+void ontc_decoder_destroy(ontc_decoder* d)
+{
+  if (!d) return;
+  cudaStreamSynchronize(d->stream);
+  release(d);
+  delete d;
+}
+
+int ontc_decode(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out)
+{
+  if (!d || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_out))) return ONTC_INVALID_STATE;
+  ontc::DecodeArgs a;
+  a.g0 = d->g0;
+  a.g1 = d->g1;
+  a.g0_words = d->g0_words;
+  a.g1_words = d->g1_words;
+  a.blob = d->blob;
+  a.k = d->k;
+  a.uv = d_uv;
+  a.lod = d_lod;
+  a.n = n;
+  a.out = d_out;
+  a.err = d->err;
+  return ontc::launch_decode(d->profile, a, d->stream) == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
+}
+
+int ontc_decoder_status(ontc_decoder* d)
+{
+  if (!d) return ONTC_INVALID_STATE;
+  int err = 0;
+  if (cudaStreamSynchronize(d->stream) != cudaSuccess ||
+      cudaMemcpy(&err, d->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return ONTC_CUDA_FAILURE;
+  return err ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int ontc_decode_host(ontc_decoder* d, const float* uv, const int32_t* lod, int64_t n, float* out)
+{
+  if (!d || n < 0 || (n > 0 && (!uv || !lod || !out))) return ONTC_INVALID_STATE;
+  if (n == 0) return ONTC_SUCCESS;
+  const int C = d->k.channel_count;
+  if (n > d->cap) {
+    cudaFree(d->uv);
+    cudaFree(d->lod);
+    cudaFree(d->out);
+    d->uv = nullptr;
+    d->lod = nullptr;
+    d->out = nullptr;
+    d->cap = 0;
+    if (cudaMalloc(&d->uv, (size_t)n * 2 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d->lod, (size_t)n * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&d->out, (size_t)n * C * sizeof(float)) != cudaSuccess)
+      return ONTC_ALLOCATION_FAILURE;
+    d->cap = n;
+  }
+  cudaError_t e = cudaMemcpyAsync(d->uv, uv, (size_t)n * 2 * sizeof(float), cudaMemcpyHostToDevice, d->stream);
+  if (!e) e = cudaMemcpyAsync(d->lod, lod, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, d->stream);
+  if (e) return ONTC_CUDA_FAILURE;
+  int r = ontc_decode(d, d->uv, d->lod, n, d->out);
+  if (r != ONTC_SUCCESS) return r;
+  if (cudaMemcpyAsync(out, d->out, (size_t)n * C * sizeof(float), cudaMemcpyDeviceToHost, d->stream) != cudaSuccess)
+    return ONTC_CUDA_FAILURE;
+  return ontc_decoder_status(d);
+}
+
+}  // extern "C"

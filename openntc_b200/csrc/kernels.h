@@ -8,9 +8,26 @@
 
 #include "common.cuh"
 
+#include "ontc.h"
+
 namespace ontc {
 
 enum { kTrain = 0, kEval = 1, kCalib = 2 };
+
+// ---- decode (SampleMaterial over a batch of samples, decode.cu)
+struct DecodeArgs {
+  const uint32_t* g0;   // packed g0 pyramid, every level at its constants offset
+  const uint32_t* g1;
+  uint32_t g0_words, g1_words;
+  const uint8_t* blob;  // int8 decoder blob (W0 | W1 | Wout | scales)
+  ontc_constants k;     // the material's NTCConstants
+  const float* uv;      // [n][2]
+  const int32_t* lod;   // [n]
+  int64_t n;
+  float* out;           // [n][k.channel_count]
+  int* err;             // set to 1 when a bounded wait gave up
+};
+cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
 
 struct TileOut {
   float* dW_partial;     // [grid][nW] per-CTA decoder gradient partial sums (kTrain)

@@ -69,6 +69,8 @@ class Oracle:
         L.orc_quantize_weights.argtypes = [P, C.c_int32, C.c_int32, C.c_float, P, P]
         L.orc_sample_material.argtypes = [C.c_int32, P, P, P, P, P, P, C.c_int64, P, C.c_int32]
         L.orc_decode_float.argtypes = [C.c_int32, P, P, P, P, C.c_int32, P, P, C.c_int64, P, C.c_int32]
+        L.orc_check_div3.argtypes = [C.c_int32]
+        L.orc_check_div3.restype = C.c_int64
         self.L = L
         self._keep = []
 

@@ -631,3 +631,25 @@ void orc_decode_float(int32_t profile, const uint32_t* g0, const uint32_t* g1, c
     }
   }
 }
+
+/* The decoder's division by 3 (RN(x * RN(1/3)) corrected once with the exact fma remainder)
+ * against IEEE division, for every float x with |x| <= 1.5 (the only range hardgelu divides
+ * in).  Returns how many x give a different value (+0 and -0 count as equal: the result is
+ * multiplied, rounded to an integer and can only become 0 either way). */
+int64_t orc_check_div3(int32_t threads)
+{
+  const float y = 1.0f / 3.0f;
+  int64_t bad = 0;
+  if (threads < 1) threads = 1;
+#pragma omp parallel for num_threads(threads) reduction(+ : bad) schedule(static)
+  for (int64_t i = 0; i < 2 * (int64_t)0x3FC00001; i++) {
+    const uint32_t b = (uint32_t)(i % 0x3FC00001) | (i >= 0x3FC00001 ? 0x80000000u : 0u);
+    float x;
+    memcpy(&x, &b, 4);
+    const float q = x * y;
+    const float r = fmaf(-q, 3.0f, x);
+    const float q1 = fmaf(r, y, q);
+    if (q1 != x / 3.0f) bad++;
+  }
+  return bad;
+}

@@ -93,6 +93,9 @@ void orc_decode_float(int32_t profile, const uint32_t* g0, const uint32_t* g1, c
                       const float* W, int32_t C, const float* uv, const int32_t* lod, int64_t n, double* out,
                       int32_t threads);
 
+/* Exhaustive check of the decoder's division by 3 (see ontc_oracle.c); returns mismatches. */
+int64_t orc_check_div3(int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif
