@@ -8,6 +8,11 @@ moments.  A "step" is one optimisation step: draw -> gather -> MLP forward/backw
 latent scatter -> Adam over the whole current latent level.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision bf16|fp32]
+  python bench.py --workload decode [--steps K] [--warmup W]
+
+The decode workload times SampleMaterial over 3840 x 2160 x 8 = 66,355,200 samples (uv uniform
+in [0,1)^2, lod uniform in 0..12 clamped to 10) of a 4096^2 9-channel Bpp_2_25 material; a
+"step" is one decode of all samples.
 
 Prints one JSON line (rank 0).  `value` is device-timed with CUDA events on the library's
 stream (max over ranks); `e2e` is the same steps through the C ABI timed on the host,
@@ -291,6 +296,113 @@ def run_ours(args):
     return out
 
 
+DECODE = {
+    "workload": "decode_4096sq_9ch_bpp2_25_n66355200", "dim": 4096, "channels": 9, "profile": "Bpp_2_25",
+    "profile_id": 3, "samples": 3840 * 2160 * 8, "lod_max": 10, "train_steps": 40, "seed": 3,
+}
+
+
+def run_decode(args):
+    """cfg 5: batch SampleMaterial on one GPU (replicas only beyond one GPU)."""
+    import numpy as np
+    import torch
+    import openntc_b200 as ont
+    from openntc_b200.synth import make_material
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    tmp = Path(tempfile.mkdtemp(prefix=f"ontc_decode_{rank}_"))
+    manifest = make_material(tmp / "set", DECODE["dim"], DECODE["seed"] + rank, DECODE["channels"])
+    ctx = ont.Context()
+    assert ctx.init(DECODE["profile_id"]) == ont.Result.Success
+    assert ctx.load_manifest(manifest) == ont.Result.Success
+    ctx.begin_training(ont.Quality.Low, 1, steps=DECODE["train_steps"])
+    assert ctx.train_until_complete().phase == ont.TrainPhase.TrainComplete
+    cd = ctx.get_compressed_data()
+    n = DECODE["samples"]
+    C = cd.channel_count
+    g = torch.Generator(device="cuda").manual_seed(DECODE["seed"])
+    uv = torch.rand((n, 2), device="cuda", generator=g)
+    lod = torch.randint(0, 13, (n,), device="cuda", generator=g, dtype=torch.int32).clamp_(max=DECODE["lod_max"])
+    out = torch.empty((n, C), device="cuda")
+    stream = torch.cuda.Stream()
+    dec = ont.Decoder(cd, stream.cuda_stream)
+    torch.cuda.synchronize()
+    K, W = args.steps, args.warmup
+    for _ in range(W):
+        assert dec.decode(uv.data_ptr(), lod.data_ptr(), n, out.data_ptr()) == 0
+    assert dec.status() == 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(K):
+            dec.decode(uv.data_ptr(), lod.data_ptr(), n, out.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    assert dec.status() == 0
+    ms = ev0.elapsed_time(ev1) / K
+    value = n / (ms / 1e3)
+    # e2e: host (pinned) samples in, host outputs back, through ontc_decode_host
+    h_uv, h_lod = uv.cpu().pin_memory(), lod.cpu().pin_memory()
+    h_out = torch.empty((n, C), pin_memory=True)
+    lib = ont.load()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        assert lib.ontc_decode_host(dec.handle, h_uv.data_ptr(), h_lod.data_ptr(), n, h_out.data_ptr()) == 0
+    e2e_s = (time.perf_counter() - t0) / 2
+    pk = peaks()
+    bytes_per = 8 + 4 + 4 * C              # uv f32 x2 + lod i32 in, C f32 out
+    ops_per = 2 * (64 * 92 + 64 * 64 + 9 * 64)  # int8 multiply-adds x 2 (F = 92 for Bpp_2_25)
+    gbs = n * bytes_per / (ms / 1e3) / 1e9
+    tops = n * ops_per / (ms / 1e3) / 1e12
+    cpu = None
+    if not args.no_cpu_baseline:
+        import ctypes
+        from oracle.bindings import Oracle
+
+        def pyramid(which):
+            total = cd.g0_total_size if which == 0 else cd.g1_total_size
+            buf = np.zeros(total // 4, np.uint32)
+            for l in range(cd.level_count):
+                ptr, size, off = ((cd.g0[l], cd.g0_size[l], cd.g0_offset[l]) if which == 0 else
+                                  (cd.g1[l], cd.g1_size[l], cd.g1_offset[l]))
+                buf[off // 4:(off + size) // 4] = np.ctypeslib.as_array(ptr, (size // 4,))
+            return buf
+
+        blob = np.ctypeslib.as_array(ctypes.cast(cd.decoder, ctypes.POINTER(ctypes.c_uint8)), (cd.decoder_size,))
+        o = Oracle()
+        k = bytes(ont.fill_constants(cd))
+        m = 1 << 20
+        threads = os.cpu_count() or 1
+        hu, hl = h_uv[:m].numpy(), h_lod[:m].numpy()
+        t0 = time.perf_counter()
+        o.sample_material(cd.profile, pyramid(0), pyramid(1), blob, k, hu, hl, C, threads=threads)
+        cs = time.perf_counter() - t0
+        cpu = {"value": round(m / cs, 1), "unit": "samples/s", "cores": threads, "kind": "port",
+               "sample": f"oracle SampleMaterial (C restatement of the DP4A path, OpenMP) on the first {m} samples"}
+    outl = {
+        "metric": "decode samples/s", "value": round(value, 1), "unit": "samples/s", "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8 (s32 accumulate, fp32 requantisation)",
+        "data": "synthetic: seeded 4096^2 9-channel PBR set trained for a short schedule; seeded uv/lod",
+        "config": dict(DECODE, l2="inputs and outputs (3.2 GB per step) are larger than L2"),
+        "roofline": {"bound": "hbm", "kernel": "decode_kernel (features, 3 int8 tcgen05 layers, requantisation)",
+                     "achieved": round(gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"], "traffic": None,
+                     "algorithmic_bytes_per_sample": bytes_per, "int8_tops": round(tops, 1),
+                     "int8_tops_peak": round(2 * pk["bf16_tflops"], 1),
+                     "note": "int8 peak taken as 2x the measured dense bf16 figure (spec ratio)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(n / e2e_s, 1), "unit": "samples/s", "h2d_bytes_per_step": n * 12,
+                "d2h_bytes_per_step": n * 4 * C, "what": "ontc_decode_host from pinned host buffers"},
+        "clocks": clk.summary(), "gpu_launches": K, "impl": "ours",
+    }
+    if rank == 0:
+        print(json.dumps(outl), flush=True)
+    del dec
+    ctx.destroy()
+    return outl
+
+
 def run_reference(args):
     world, rank, local = dist_setup(args)
     if rank != 0:
@@ -346,9 +458,16 @@ def main():
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
     ap.add_argument("--latent-adam", choices=["deferred", "dense"], default="deferred")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["train", "decode"], default="train")
     args = ap.parse_args()
     assert args.warmup >= 3
-    if args.impl == "reference":
+    if args.workload == "decode":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "upstream decodes in HLSL only "
+                              "(ntc_decode.hlsli); no graphics stack or DXC on this box"}))
+        else:
+            run_decode(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

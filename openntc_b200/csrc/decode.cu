@@ -27,11 +27,12 @@ namespace ontc {
 
 namespace {
 
-constexpr int kGroups = 4;
+constexpr int kGroups = 8;  // 1024 threads, 64 registers each; 8 x 64 TMEM columns
 constexpr int kGroupThreads = 128;
 constexpr int kThreads = kGroups * kGroupThreads;
 constexpr int kHid = 64;
 constexpr int kOutRows = 16;  // upstream's padded output rows (OUTP)
+static_assert(64 * kGroups == 512 || 64 * kGroups == 256 || 64 * kGroups == 128, "TMEM allocations are powers of two");
 
 // Compile-time profile shape (ntc_decode.hlsli:60-86): channels, bits, first-level mips.
 template <int C0_, int C1_, int B0_, int B1_, int L0MIPS_>
@@ -78,6 +79,30 @@ template <int B>
 __device__ __forceinline__ uint32_t code_of(const uint32_t* s, int c)
 {
   return (s[(c * B) >> 5] >> ((c * B) & 31)) & ((1u << B) - 1u);
+}
+
+// Four consecutive B-bit codes starting at channel c (4 | c) as four signed feature bytes,
+// (code << (8 - B)) ^ 0x80 each, built with word-wide shifts and byte permutes.
+template <int B>
+__device__ __forceinline__ uint32_t code_bytes4(const uint32_t* s, int c)
+{
+  const uint32_t t = s[(c * B) >> 5] >> ((c * B) & 31);  // codes c..c+3 in the low 4B bits
+  if constexpr (B == 4) {
+    const uint32_t lo = t & 0x0F0Fu, hi = (t >> 4) & 0x0F0Fu;   // n0 n2 | n1 n3
+    const uint32_t n = __byte_perm(lo, hi, 0x5140);             // n0 n1 n2 n3
+    return ((n << 4) & 0xF0F0F0F0u) ^ 0x80808080u;
+  } else {
+    static_assert(B == 2, "2- or 4-bit g0 codes");
+    const uint32_t t8 = t & 0xFFu;  // exactly the four codes: higher ones would land on the targets
+    const uint32_t u = (t8 << 6) | (t8 << 12) | (t8 << 18) | (t8 << 24);  // code k -> bits 8k+6..8k+7
+    return (u & 0xC0C0C0C0u) ^ 0x80808080u;
+  }
+}
+
+// (float)code for a small non-negative integer code, without a conversion instruction.
+__device__ __forceinline__ float code_float(uint32_t code)
+{
+  return __fsub_rn(__uint_as_float(0x4B000000u | code), 8388608.0f);
 }
 
 // ClampS8(round(f)) with HLSL round = nearest, ties to even.  Clamping first leaves the
@@ -133,11 +158,9 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
       const int cx = clampi(gx + (q & 1), 0, d0 - 1), cy = clampi(gy + (q >> 1), 0, d0 - 1);
       uint32_t st[(C0 * B0 + 31) / 32];
       cell_stream<C0 * B0>(A.g0, A.g0_words, o0, (uint32_t)(cy * d0 + cx), st);
+      static_assert(C0 % 4 == 0, "g0 features fill whole words");
 #pragma unroll
-      for (int c = 0; c < C0; c++) {
-        const uint32_t code = code_of<B0>(st, c);
-        put_byte(w, q * C0 + c, (int)((code << (8 - B0)) ^ 0x80u));
-      }
+      for (int c = 0; c < C0; c += 4) w[(q * C0 + c) >> 2] = code_bytes4<B0>(st, c);
     }
   }
   // g1: bilinear blend of the dequantised codes, then *128 to a signed byte
@@ -149,7 +172,9 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
     const float fx = __fsub_rn(g1x, flx), fy = __fsub_rn(g1y, fly);
     const float ofx = __fsub_rn(1.0f, fx), ofy = __fsub_rn(1.0f, fy);
     const float mult[4] = {__fmul_rn(ofx, ofy), __fmul_rn(fx, ofy), __fmul_rn(ofx, fy), __fmul_rn(fx, fy)};
-    const float half = (float)(1u << (B1 - 1));
+    // ((float)code - half) / half: half is a power of two, so the division is the exact
+    // multiplication by 1 / half
+    const float half = (float)(1u << (B1 - 1)), rhalf = 1.0f / half;
     float blend[C1];
 #pragma unroll
     for (int c = 0; c < C1; c++) blend[c] = 0.0f;
@@ -161,7 +186,7 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
 #pragma unroll
       for (int c = 0; c < C1; c++) {
         const uint32_t code = code_of<B1>(st, c);
-        blend[c] = __fmaf_rn(mult[q], __fdiv_rn(__fsub_rn((float)code, half), half), blend[c]);
+        blend[c] = __fmaf_rn(mult[q], __fmul_rn(__fsub_rn(code_float(code), half), rhalf), blend[c]);
       }
     }
 #pragma unroll
@@ -177,10 +202,10 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
       for (int a = 0; a < 2; a++)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const float P = (float)(8 >> p);
+          const float P = (float)(8 >> p), rP = 1.0f / P;  // P = 8, 4, 2: dividing = exact scaling
           const float c = a == 0 ? tcx : tcy;
           const float ph = h == 0 ? 0.0f : __fmul_rn(0.25f, P);
-          const float t = __fdiv_rn(__fadd_rn(__fadd_rn(c, 0.5f), ph), P);
+          const float t = __fmul_rn(__fadd_rn(__fadd_rn(c, 0.5f), ph), rP);
           const float pe = __fsub_rn(1.0f, __fmul_rn(4.0f, fabsf(__fsub_rn(__fsub_rn(t, floorf(t)), 0.5f))));
           put_byte(w, 4 * C0 + C1 + p * 4 + a * 2 + h, q8(__fmul_rn(pe, 128.0f)));
         }
@@ -261,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
     ptx::fence_mbar_init();
     fail_s = 0;
   }
-  if (warp == 0) ptx::tmem_alloc(&tmem_base_s, 64 * kGroups);
+  if (warp == 0) ptx::tmem_alloc(&tmem_base_s, 64 * kGroups);  // a power of two: 512
   load_decoder<SH>(A.blob, sW0, sW1, sWo, s0, s1, so);
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
