@@ -99,12 +99,6 @@ __device__ __forceinline__ uint32_t code_bytes4(const uint32_t* s, int c)
   }
 }
 
-// (float)code for a small non-negative integer code, without a conversion instruction.
-__device__ __forceinline__ float code_float(uint32_t code)
-{
-  return __fsub_rn(__uint_as_float(0x4B000000u | code), 8388608.0f);
-}
-
 // ClampS8(round(f)) with HLSL round = nearest, ties to even.  Clamping first leaves the
 // result unchanged (rounding is monotonic and the bounds are integers) and keeps |f| < 2^22,
 // where adding 1.5 * 2^23 rounds to an integer in the low mantissa bits.
@@ -112,6 +106,18 @@ __device__ __forceinline__ int q8(float f)
 {
   f = fminf(fmaxf(f, -128.0f), 127.0f);
   return __float_as_int(__fadd_rn(f, 12582912.0f)) - 0x4B400000;
+}
+// The same rounded value k in [-128, 127] as the float bits 0x4B400000 + k, whose low byte is
+// k's two's-complement byte (0x4B400000 has 22 zero low bits): pack bytes without subtracting.
+__device__ __forceinline__ uint32_t q8_bits(float f)
+{
+  f = fminf(fmaxf(f, -128.0f), 127.0f);
+  return __float_as_uint(__fadd_rn(f, 12582912.0f));
+}
+// Low bytes of four words -> one word (byte i from word i).
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
 // x / 3 correctly rounded: RN(x * RN(1/3)) corrected once with the exact remainder
@@ -125,11 +131,14 @@ __device__ __forceinline__ float div3(float x)
   return __fmaf_rn(r, y, q);
 }
 
-// hardgelu4 (ntc_decode.hlsli:400-403): x < -1.5 ? 0 : x < 1.5 ? (x / 3) * (x + 1.5) : x
+// hardgelu4 (ntc_decode.hlsli:400-403): x < -1.5 ? 0 : x < 1.5 ? (x / 3) * (x + 1.5) : x.
+// Below -1.5 the middle formula at -1.5 gives (-0.5) * 0 = -0, which scales and rounds to the
+// same 0, so the lower branch is a max.
 __device__ __forceinline__ float hg_hlsl(float x)
 {
-  const float mid = __fmul_rn(div3(x), __fadd_rn(x, 1.5f));
-  return x < -1.5f ? 0.0f : (x < 1.5f ? mid : x);
+  const float c = fmaxf(x, -1.5f);
+  const float mid = __fmul_rn(div3(c), __fadd_rn(c, 1.5f));
+  return x < 1.5f ? mid : x;
 }
 
 __device__ __forceinline__ void put_byte(uint32_t* w, int f, int v)
@@ -172,9 +181,11 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
     const float fx = __fsub_rn(g1x, flx), fy = __fsub_rn(g1y, fly);
     const float ofx = __fsub_rn(1.0f, fx), ofy = __fsub_rn(1.0f, fy);
     const float mult[4] = {__fmul_rn(ofx, ofy), __fmul_rn(fx, ofy), __fmul_rn(ofx, fy), __fmul_rn(fx, fy)};
-    // ((float)code - half) / half: half is a power of two, so the division is the exact
-    // multiplication by 1 / half
+    // mult * (((float)code - half) / half): code - half is exact, and half is a power of two,
+    // so the exact product is (mult / half) * (code - half) with mult / half exact too
     const float half = (float)(1u << (B1 - 1)), rhalf = 1.0f / half;
+    const float mh[4] = {__fmul_rn(mult[0], rhalf), __fmul_rn(mult[1], rhalf), __fmul_rn(mult[2], rhalf),
+                         __fmul_rn(mult[3], rhalf)};
     float blend[C1];
 #pragma unroll
     for (int c = 0; c < C1; c++) blend[c] = 0.0f;
@@ -186,7 +197,8 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
 #pragma unroll
       for (int c = 0; c < C1; c++) {
         const uint32_t code = code_of<B1>(st, c);
-        blend[c] = __fmaf_rn(mult[q], __fmul_rn(__fsub_rn(code_float(code), half), rhalf), blend[c]);
+        const float centred = __fsub_rn(__uint_as_float(0x4B000000u | code), 8388608.0f + half);  // code - half
+        blend[c] = __fmaf_rn(mh[q], centred, blend[c]);
       }
     }
 #pragma unroll
@@ -227,14 +239,14 @@ __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restric
   float acc[16];
   ptx::ld16(taddr, acc);
   ptx::ld_wait();
-#pragma unroll
-  for (int i = 0; i < 4; i++) out[i] = 0u;
+  uint32_t b[16];
 #pragma unroll
   for (int j = 0; j < 16; j++) {
     const float x = __fmul_rn((float)__float_as_int(acc[j]), scale[j]);
-    const int a = q8(__fmul_rn(hg_hlsl(x), rcp));
-    out[j >> 2] |= ((uint32_t)a & 0xFFu) << (8 * (j & 3));
+    b[j] = q8_bits(__fmul_rn(hg_hlsl(x), rcp));
   }
+#pragma unroll
+  for (int i = 0; i < 4; i++) out[i] = pack4(b[4 * i], b[4 * i + 1], b[4 * i + 2], b[4 * i + 3]);
 }
 
 template <class SH>
