@@ -107,98 +107,104 @@ __device__ __forceinline__ void decoder_block(const Model& M, const StepRec& s, 
 // dense update would have applied them (same adam1 arithmetic, same clamp), only later: right
 // before the cell is read again (catch-up over the step's footprint) or in a level sweep.
 
-// The C latents of one cell (contiguous, 8- or 16-byte aligned: C is even, buffers 256-byte).
+// Each cell's C channels are split into groups of W = 4 (float4) or, when C is not a multiple
+// of 4, W = 2 (float2); one thread takes one (cell, group), so a footprint of n cells runs
+// n * C / W threads.
 template <int C>
-__device__ __forceinline__ void load_cell(const float* __restrict__ src, int64_t e, float (&x)[C])
+struct Groups {
+  static constexpr int W = (C % 4 == 0) ? 4 : 2;
+  static constexpr int Q = C / W;
+};
+
+template <int W>
+__device__ __forceinline__ void load_grp(const float* __restrict__ src, int64_t e, float (&x)[W])
 {
-  if constexpr (C % 4 == 0) {
-#pragma unroll
-    for (int k = 0; k < C / 4; k++) {
-      const float4 t = reinterpret_cast<const float4*>(src + e)[k];
-      x[4 * k] = t.x, x[4 * k + 1] = t.y, x[4 * k + 2] = t.z, x[4 * k + 3] = t.w;
-    }
+  if constexpr (W == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(src + e);
+    x[0] = t.x, x[1] = t.y, x[2] = t.z, x[3] = t.w;
   } else {
-    static_assert(C % 2 == 0, "latent channel counts are even");
-#pragma unroll
-    for (int k = 0; k < C / 2; k++) {
-      const float2 t = reinterpret_cast<const float2*>(src + e)[k];
-      x[2 * k] = t.x, x[2 * k + 1] = t.y;
-    }
+    const float2 t = *reinterpret_cast<const float2*>(src + e);
+    x[0] = t.x, x[1] = t.y;
   }
 }
 
-template <int C>
-__device__ __forceinline__ void store_cell(float* __restrict__ dst, int64_t e, const float (&x)[C])
+template <int W>
+__device__ __forceinline__ void store_grp(float* __restrict__ dst, int64_t e, const float (&x)[W])
 {
-  if constexpr (C % 4 == 0) {
-#pragma unroll
-    for (int k = 0; k < C / 4; k++)
-      reinterpret_cast<float4*>(dst + e)[k] = make_float4(x[4 * k], x[4 * k + 1], x[4 * k + 2], x[4 * k + 3]);
-  } else {
-#pragma unroll
-    for (int k = 0; k < C / 2; k++) reinterpret_cast<float2*>(dst + e)[k] = make_float2(x[2 * k], x[2 * k + 1]);
-  }
+  if constexpr (W == 4)
+    *reinterpret_cast<float4*>(dst + e) = make_float4(x[0], x[1], x[2], x[3]);
+  else
+    *reinterpret_cast<float2*>(dst + e) = make_float2(x[0], x[1]);
 }
 
-// Replays level steps [a, J) with zero gradient on every channel of `cell`; the C channel
-// chains are independent, so they interleave.
-template <int C>
-__device__ __forceinline__ void replay_cell(const Pyramid& P, int lvl, int cell, int a, int J,
-                                            const float4* __restrict__ hist)
+// Replays level steps [a, J) with zero gradient on the W latents at offset e.
+template <int W>
+__device__ __forceinline__ void replay_grp(const Pyramid& P, int lvl, int64_t e, int a, int J,
+                                           const float4* __restrict__ hist)
 {
-  const int64_t e = (int64_t)cell * C;
-  float p[C], m[C], v[C];
-  load_cell<C>(P.p[lvl], e, p);
-  load_cell<C>(P.m[lvl], e, m);
-  load_cell<C>(P.v[lvl], e, v);
+  float p[W], m[W], v[W];
+  load_grp<W>(P.p[lvl], e, p);
+  load_grp<W>(P.m[lvl], e, m);
+  load_grp<W>(P.v[lvl], e, v);
   for (int t = a; t < J; t++) {
     const float4 h = hist[t & (kHistRing - 1)];
 #pragma unroll
-    for (int c = 0; c < C; c++) {
+    for (int c = 0; c < W; c++) {
       adam1(p[c], m[c], v[c], 0.0f, h.x, h.y, h.z);
       p[c] = clamp_latent(p[c], P.delta);
     }
   }
-  store_cell<C>(P.p[lvl], e, p);
-  store_cell<C>(P.m[lvl], e, m);
-  store_cell<C>(P.v[lvl], e, v);
+  store_grp<W>(P.p[lvl], e, p);
+  store_grp<W>(P.m[lvl], e, m);
+  store_grp<W>(P.v[lvl], e, v);
 }
 
-// Applies the step's gradient to every channel of `cell` and clears it.
-template <int C>
-__device__ __forceinline__ void update_cell(const Pyramid& P, int lvl, int cell, float lr, float b1, float b2)
+// Applies the step's gradient to the W latents at offset e and clears it.
+template <int W>
+__device__ __forceinline__ void update_grp(const Pyramid& P, int lvl, int64_t e, float lr, float b1, float b2)
 {
-  const int64_t e = (int64_t)cell * C;
-  float p[C], m[C], v[C], g[C];
-  load_cell<C>(P.p[lvl], e, p);
-  load_cell<C>(P.m[lvl], e, m);
-  load_cell<C>(P.v[lvl], e, v);
-  load_cell<C>(P.g[lvl], e, g);
+  float p[W], m[W], v[W], g[W];
+  load_grp<W>(P.p[lvl], e, p);
+  load_grp<W>(P.m[lvl], e, m);
+  load_grp<W>(P.v[lvl], e, v);
+  load_grp<W>(P.g[lvl], e, g);
 #pragma unroll
-  for (int c = 0; c < C; c++) {
+  for (int c = 0; c < W; c++) {
     adam1(p[c], m[c], v[c], g[c], lr, b1, b2);
     p[c] = clamp_latent(p[c], P.delta);
     g[c] = 0.0f;
   }
-  store_cell<C>(P.p[lvl], e, p);
-  store_cell<C>(P.m[lvl], e, m);
-  store_cell<C>(P.v[lvl], e, v);
-  store_cell<C>(P.g[lvl], e, g);
+  store_grp<W>(P.p[lvl], e, p);
+  store_grp<W>(P.m[lvl], e, m);
+  store_grp<W>(P.v[lvl], e, v);
+  store_grp<W>(P.g[lvl], e, g);
 }
 
-// Footprint cell `i` of F -> pyramid g and cell index in the level.
-__device__ __forceinline__ bool foot_cell(const FootRec& F, int i, const Model& M, int lvl, int& g, int& cell)
+// Footprint work item i of F -> pyramid g, cell index in the level and channel group q.
+template <int C0, int C1>
+__device__ __forceinline__ bool foot_item(const FootRec& F, int i, const Model& M, int lvl, int& g, int& cell,
+                                          int& q)
 {
-  g = i < F.cells[0] ? 0 : 1;
-  const int local = g ? i - F.cells[0] : i;
-  if (g == 1 && local >= F.cells[1]) return false;
+  constexpr int Q0 = Groups<C0>::Q, Q1 = Groups<C1>::Q;
+  const int n0 = F.cells[0] * Q0;
+  g = i < n0 ? 0 : 1;
+  int local;
+  if (g == 0) {
+    local = i / Q0;
+    q = i - local * Q0;
+  } else {
+    const int j = i - n0;
+    if (j >= F.cells[1] * Q1) return false;
+    local = j / Q1;
+    q = j - local * Q1;
+  }
   int r = 0;
   for (int k = 1; k < F.n[g]; k++) r = F.start[g][k] <= local ? k : r;
   const int w = F.r[g][r][2];
-  const int q = local - F.start[g][r];
-  const int row = q / w;
+  const int off = local - F.start[g][r];
+  const int row = off / w;
   const int dim = g == 0 ? M.g0.dim[lvl] : M.g1.dim[lvl];
-  cell = (F.r[g][r][1] + row) * dim + F.r[g][r][0] + (q - row * w);
+  cell = (F.r[g][r][1] + row) * dim + F.r[g][r][0] + (off - row * w);
   return true;
 }
 
@@ -209,37 +215,40 @@ __global__ void __launch_bounds__(256) catchup_kernel(Model M, const StepRec* __
   const StepRec& s = steps[idx];
   const int lvl = s.level, j = s.gstep, fl = s.gfloor;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int g, cell;
-  if (!foot_cell(F, i, M, lvl, g, cell)) return;
+  int g, cell, q;
+  if (!foot_item<C0, C1>(F, i, M, lvl, g, cell, q)) return;
   const int a = max(M.applied[g][lvl][cell], fl);
   if (a >= j) return;
   if (g == 0)
-    replay_cell<C0>(M.g0, lvl, cell, a, j, M.hist[lvl]);
+    replay_grp<Groups<C0>::W>(M.g0, lvl, (int64_t)cell * C0 + q * Groups<C0>::W, a, j, M.hist[lvl]);
   else
-    replay_cell<C1>(M.g1, lvl, cell, a, j, M.hist[lvl]);
+    replay_grp<Groups<C1>::W>(M.g1, lvl, (int64_t)cell * C1 + q * Groups<C1>::W, a, j, M.hist[lvl]);
 }
 
-// Brings every cell of level `lvl` from max(applied, fl) up to J.  Writes no counter: the
+// Brings every latent of level `lvl` from max(applied, fl) up to J.  Writes no counter: the
 // caller raises the level's floor to J.
 template <int C0, int C1>
 __global__ void __launch_bounds__(256) sweep_kernel(Model M, int lvl, int fl, int J)
 {
-  const int n0 = M.g0.dim[lvl] * M.g0.dim[lvl];
-  const int n1 = M.g1.dim[lvl] * M.g1.dim[lvl];
+  constexpr int Q0 = Groups<C0>::Q, Q1 = Groups<C1>::Q;
+  const int n0 = M.g0.dim[lvl] * M.g0.dim[lvl] * Q0;
+  const int n1 = M.g1.dim[lvl] * M.g1.dim[lvl] * Q1;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0 + n1; i += gridDim.x * blockDim.x) {
-    const int g = i < n0 ? 0 : 1;
-    const int cell = g ? i - n0 : i;
-    const int a = max(M.applied[g][lvl][cell], fl);
-    if (a >= J) continue;
-    if (g == 0)
-      replay_cell<C0>(M.g0, lvl, cell, a, J, M.hist[lvl]);
-    else
-      replay_cell<C1>(M.g1, lvl, cell, a, J, M.hist[lvl]);
+    if (i < n0) {
+      const int cell = i / Q0, q = i - cell * Q0;
+      const int a = max(M.applied[0][lvl][cell], fl);
+      if (a < J) replay_grp<Groups<C0>::W>(M.g0, lvl, (int64_t)cell * C0 + q * Groups<C0>::W, a, J, M.hist[lvl]);
+    } else {
+      const int k = i - n0;
+      const int cell = k / Q1, q = k - cell * Q1;
+      const int a = max(M.applied[1][lvl][cell], fl);
+      if (a < J) replay_grp<Groups<C1>::W>(M.g1, lvl, (int64_t)cell * C1 + q * Groups<C1>::W, a, J, M.hist[lvl]);
+    }
   }
 }
 
-// Decoder Adam (CTAs [0, n_dec)) and the step's gradient on its footprint, every cell of which
-// is at level step gstep (the other CTAs).
+// Decoder Adam (CTAs [0, n_dec)) and the step's gradient on its footprint, every latent of
+// which is at level step gstep (the other CTAs).
 template <int C0, int C1>
 __global__ void __launch_bounds__(256) footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx,
                                                                const __grid_constant__ FootRec F,
@@ -255,13 +264,13 @@ __global__ void __launch_bounds__(256) footprint_update_kernel(Model M, const St
   const int lvl = s.level, j = s.gstep;
   const int i = (blockIdx.x - n_dec) * blockDim.x + threadIdx.x;
   if (i == 0) M.hist[lvl][j & (kHistRing - 1)] = make_float4(s.lr_grid, s.gb1, s.gb2, 0.0f);
-  int g, cell;
-  if (!foot_cell(F, i, M, lvl, g, cell)) return;
+  int g, cell, q;
+  if (!foot_item<C0, C1>(F, i, M, lvl, g, cell, q)) return;
   if (g == 0)
-    update_cell<C0>(M.g0, lvl, cell, s.lr_grid, s.gb1, s.gb2);
+    update_grp<Groups<C0>::W>(M.g0, lvl, (int64_t)cell * C0 + q * Groups<C0>::W, s.lr_grid, s.gb1, s.gb2);
   else
-    update_cell<C1>(M.g1, lvl, cell, s.lr_grid, s.gb1, s.gb2);
-  M.applied[g][lvl][cell] = j + 1;
+    update_grp<Groups<C1>::W>(M.g1, lvl, (int64_t)cell * C1 + q * Groups<C1>::W, s.lr_grid, s.gb1, s.gb2);
+  if (q == 0) M.applied[g][lvl][cell] = j + 1;  // no thread of this kernel reads the counters
 }
 
 __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* __restrict__ steps, int step_idx,
@@ -352,12 +361,12 @@ static int dec_blocks(const Model& M) { return (M.nW + 31) / 32; }
 cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
                            cudaStream_t stream)
 {
-  const int total = F.cells[0] + F.cells[1];
-  if (total <= 0) return cudaSuccess;
-#define X(a, b)                                                                          \
-  if (M.g0.channels == a && M.g1.channels == b) {                                        \
-    catchup_kernel<a, b><<<(total + 255) / 256, 256, 0, stream>>>(M, d_steps, step_idx, F); \
-    return cudaGetLastError();                                                           \
+#define X(a, b)                                                                                          \
+  if (M.g0.channels == a && M.g1.channels == b) {                                                        \
+    const int total = F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q;                             \
+    if (total <= 0) return cudaSuccess;                                                                  \
+    catchup_kernel<a, b><<<(total + 255) / 256, 256, 0, stream>>>(M, d_steps, step_idx, F);             \
+    return cudaGetLastError();                                                                           \
   }
   ONTC_FOR_CHANNEL_PAIRS(X)
 #undef X
@@ -368,11 +377,11 @@ cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int 
                                     const float* dW_partial, const double* loss_partial, int grid,
                                     double* loss_out, cudaStream_t stream)
 {
-  const int total = std::max(1, F.cells[0] + F.cells[1]);
   const int n_dec = dec_blocks(M);
-  const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);
 #define X(a, b)                                                                                          \
   if (M.g0.channels == a && M.g1.channels == b) {                                                        \
+    const int total = std::max(1, F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q);                \
+    const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                     \
     footprint_update_kernel<a, b><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, loss_partial, \
                                                               grid, loss_out, n_dec);                    \
     return cudaGetLastError();                                                                           \
@@ -384,13 +393,13 @@ cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int 
 
 cudaError_t launch_sweep(const Model& M, int level, int from, int J, cudaStream_t stream)
 {
-  const long long n = (long long)M.g0.dim[level] * M.g0.dim[level] + (long long)M.g1.dim[level] * M.g1.dim[level];
-  long long blocks = (n + 255) / 256;
-  if (blocks > (long long)sm_count() * 8) blocks = (long long)sm_count() * 8;
-#define X(a, b)                                                                          \
-  if (M.g0.channels == a && M.g1.channels == b) {                                        \
-    sweep_kernel<a, b><<<(unsigned)blocks, 256, 0, stream>>>(M, level, from, J);         \
-    return cudaGetLastError();                                                           \
+#define X(a, b)                                                                                          \
+  if (M.g0.channels == a && M.g1.channels == b) {                                                        \
+    const long long n = (long long)M.g0.dim[level] * M.g0.dim[level] * Groups<a>::Q +                    \
+                        (long long)M.g1.dim[level] * M.g1.dim[level] * Groups<b>::Q;                     \
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)sm_count() * 16);           \
+    sweep_kernel<a, b><<<(unsigned)blocks, 256, 0, stream>>>(M, level, from, J);                         \
+    return cudaGetLastError();                                                                           \
   }
   ONTC_FOR_CHANNEL_PAIRS(X)
 #undef X
