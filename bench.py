@@ -254,7 +254,8 @@ def run_ours(args):
         "catchup": {"name": "catchup_kernel + sweep_kernel (zero-gradient replay)", "bound": "hbm",
                     "achieved": round(gbs(catchup), 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "launches_per_step": catchup.launches / K, "avg_launch_us": per_launch(catchup),
-                    "share_of_step": round(catchup.total_ms / step_total, 3), "traffic": None},
+                    "share_of_step": round(catchup.total_ms / step_total, 3),
+                    "traffic": traffic_tab.get("catchup_bytes_per_launch")},
     }
     for k in kernels.values():
         k["frac"] = round(k["achieved"] / k["peak"], 4) if k["peak"] else None
@@ -311,14 +312,17 @@ def run_decode(args):
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     tmp = Path(tempfile.mkdtemp(prefix=f"ontc_decode_{rank}_"))
-    manifest = make_material(tmp / "set", DECODE["dim"], DECODE["seed"] + rank, DECODE["channels"])
+    cfg = dict(DECODE, dim=args.decode_dim or DECODE["dim"], samples=args.decode_samples or DECODE["samples"])
+    if cfg != DECODE:
+        cfg["workload"] = f"decode_{cfg['dim']}sq_9ch_bpp2_25_n{cfg['samples']}"
+    manifest = make_material(tmp / "set", cfg["dim"], DECODE["seed"] + rank, DECODE["channels"])
     ctx = ont.Context()
     assert ctx.init(DECODE["profile_id"]) == ont.Result.Success
     assert ctx.load_manifest(manifest) == ont.Result.Success
     ctx.begin_training(ont.Quality.Low, 1, steps=DECODE["train_steps"])
     assert ctx.train_until_complete().phase == ont.TrainPhase.TrainComplete
     cd = ctx.get_compressed_data()
-    n = DECODE["samples"]
+    n = cfg["samples"]
     C = cd.channel_count
     g = torch.Generator(device="cuda").manual_seed(DECODE["seed"])
     uv = torch.rand((n, 2), device="cuda", generator=g)
@@ -384,7 +388,7 @@ def run_decode(args):
         "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8 (s32 accumulate, fp32 requantisation)",
         "data": "synthetic: seeded 4096^2 9-channel PBR set trained for a short schedule; seeded uv/lod",
-        "config": dict(DECODE, l2="inputs and outputs (3.2 GB per step) are larger than L2"),
+        "config": dict(cfg, l2=f"inputs and outputs ({n * (12 + 4 * C) / 1e9:.2f} GB per step) vs 0.126 GB of L2"),
         "roofline": {"bound": "hbm", "kernel": "decode_kernel (features, 3 int8 tcgen05 layers, requantisation)",
                      "achieved": round(gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"], "traffic": None,
@@ -459,6 +463,8 @@ def main():
     ap.add_argument("--latent-adam", choices=["deferred", "dense"], default="deferred")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["train", "decode"], default="train")
+    ap.add_argument("--decode-dim", type=int, default=0, help="decode material size (default 4096)")
+    ap.add_argument("--decode-samples", type=int, default=0, help="samples per decode (default 66,355,200)")
     args = ap.parse_args()
     assert args.warmup >= 3
     if args.workload == "decode":
