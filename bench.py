@@ -93,10 +93,8 @@ class Clocks:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from openntc_b200.replicas import env_rank
+    return env_rank()
 
 
 def make_set(base: Path, seed: int) -> Path:
@@ -147,16 +145,14 @@ def run_ours(args):
     import ctypes as C
 
     import torch
-    import torch.distributed as dist
 
     import openntc_b200 as ont
     from openntc_b200 import _abi
+    from openntc_b200.replicas import ReplicaGroup
 
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    group = ReplicaGroup(world, rank)  # replicas: host-side exchange of timings only
     tmp = Path(tempfile.mkdtemp(prefix=f"ontc_bench_{rank}_"))
     manifest = make_set(tmp, WORKLOAD["seed"] + rank)  # weak scaling: one material per rank
     stream = torch.cuda.Stream()
@@ -172,16 +168,8 @@ def run_ours(args):
     assert W + 3 * K + 1 < int(0.95 * WORKLOAD["schedule_steps"]), "timed steps must stay before the latent lock"
     B = WORKLOAD["batch_texels"]
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = group.barrier
+    max_over_ranks = group.max
 
     p = ctx.train(W)
     assert p.result == 0, p
@@ -291,9 +279,8 @@ def run_ours(args):
         }
         print(json.dumps(out), flush=True)
     ctx.destroy()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.barrier()
+    group.close()
     return out
 
 
