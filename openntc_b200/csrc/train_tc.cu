@@ -108,6 +108,49 @@ __device__ __forceinline__ float hg_grad_fast(float x)
   return x < -1.5f ? 0.0f : (x < 1.5f ? (2.0f * x + 1.5f) * (1.0f / 3.0f) : 1.0f);
 }
 
+// The step's level as the tile kernel uses it: resolved once per CTA into shared memory (the
+// Model's per-level arrays are kernel parameters indexed by a runtime level), and passed by
+// value to the out-of-line paths.
+struct LevelArgs {
+  const float* p0;
+  const float* p1;
+  float* g0;
+  float* g1;
+  const float* n0;  // upstream-mode noise buffers
+  const float* n1;
+  float delta0, delta1, norm_lod;
+  uint32_t seed;
+  int d0, d1, mip_dim, noise;
+};
+
+__device__ __forceinline__ LevelArgs level_args(const Model& M, const StepRec& s)
+{
+  LevelArgs L;
+  L.p0 = M.g0.p[s.level];
+  L.p1 = M.g1.p[s.level];
+  L.g0 = M.g0.g[s.level];
+  L.g1 = M.g1.g[s.level];
+  L.n0 = M.noise0;
+  L.n1 = M.noise1;
+  L.delta0 = M.g0.delta;
+  L.delta1 = M.g1.delta;
+  L.norm_lod = s.norm_lod;
+  L.seed = s.seed;
+  L.d0 = M.g0.dim[s.level];
+  L.d1 = M.g1.dim[s.level];
+  L.mip_dim = s.mip_dim;
+  L.noise = s.noise;
+  return L;
+}
+
+// latent_noise (common.cuh) for the out-of-line paths
+__device__ __forceinline__ float level_noise(const LevelArgs& L, uint32_t which, uint32_t e)
+{
+  if (L.noise == 1) return noise_value(L.seed, which, e, which == 0 ? L.delta0 : L.delta1);
+  if (L.noise == 2) return which == 0 ? L.n0[e] : L.n1[e];
+  return 0.0f;
+}
+
 // ---- latent footprint of a unit ---------------------------------------------------------
 struct Foot {
   int x0, y0, w, h;
@@ -125,7 +168,7 @@ __device__ __forceinline__ void foot_span(int a, int b, int mip, int gd, int& lo
 
 // True when the unit is a 16x8 texel block that does not wrap and whose g0/g1 boxes fit.
 template <class SH>
-__device__ __forceinline__ bool unit_footprint(const Model& M, const StepRec& s, int unit, Foot& f0, Foot& f1)
+__device__ __forceinline__ bool unit_footprint(const LevelArgs& L, const StepRec& s, int unit, Foot& f0, Foot& f1)
 {
   const int lt = log2_pow2(s.tile_dim);
   if (lt < 4) return false;
@@ -135,7 +178,7 @@ __device__ __forceinline__ bool unit_footprint(const Model& M, const StepRec& s,
   const int xa = (((blk & ((1 << lb) - 1)) << 4) + s.ox[gi]) & mask;
   const int ya = (((blk >> lb) << 3) + s.oy[gi]) & mask;
   if (xa + 16 > s.mip_dim || ya + 8 > s.mip_dim) return false;
-  const int d0 = M.g0.dim[s.level], d1 = M.g1.dim[s.level];
+  const int d0 = L.d0, d1 = L.d1;
   foot_span(xa, xa + 15, s.mip_dim, d0, f0.x0, f0.w);
   foot_span(ya, ya + 7, s.mip_dim, d0, f0.y0, f0.h);
   foot_span(xa, xa + 15, s.mip_dim, d1, f1.x0, f1.w);
@@ -192,15 +235,13 @@ __device__ __forceinline__ void build_masks(const StepRec& s, int d0, int d1, co
 // copies elements gt, gt + 256, ...; add_noise then treats the same elements, so each thread
 // only needs its own copies complete.
 template <class SH>
-__device__ __forceinline__ void stage_copy(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
-                                           float* foot, int gt)
+__device__ __forceinline__ void stage_copy(const LevelArgs& L, const Foot& f0, const Foot& f1, float* foot, int gt)
 {
-  const int lvl = s.level;
   {
     constexpr int C0 = SH::C0;
-    const int d0 = M.g0.dim[lvl];
+    const int d0 = L.d0;
     const int rowq = f0.w * (C0 / 4);
-    const float* p0 = M.g0.p[lvl];
+    const float* p0 = L.p0;
     for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
       const int r = v / rowq, q = v - r * rowq;
       ptx::cp_async16(foot + r * f0.w * C0 + q * 4, p0 + ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4);
@@ -208,9 +249,9 @@ __device__ __forceinline__ void stage_copy(const Model& M, const StepRec& s, con
   }
   {
     constexpr int C1 = SH::C1;
-    const int d1 = M.g1.dim[lvl];
+    const int d1 = L.d1;
     const int rowh = f1.w * (C1 / 2);
-    const float* p1 = M.g1.p[lvl];
+    const float* p1 = L.p1;
     float* foot1 = foot + f0.w * f0.h * SH::C0;
     for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
       const int r = v / rowh, q = v - r * rowh;
@@ -221,29 +262,27 @@ __device__ __forceinline__ void stage_copy(const Model& M, const StepRec& s, con
 
 // Adds this step's quantisation noise to the staged latents this thread copied.
 template <class SH>
-__device__ __forceinline__ void stage_noise(const Model& M, const StepRec& s, const Foot& f0, const Foot& f1,
-                                            float* foot, int gt)
+__device__ __forceinline__ void stage_noise(const LevelArgs& L, const Foot& f0, const Foot& f1, float* foot, int gt)
 {
-  const int lvl = s.level;
   {
     constexpr int C0 = SH::C0;
-    const int d0 = M.g0.dim[lvl];
+    const int d0 = L.d0;
     const int rowq = f0.w * (C0 / 4);
     for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
       const int r = v / rowq, q = v - r * rowq;
       const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
       float4* dst = reinterpret_cast<float4*>(foot + r * f0.w * C0 + q * 4);
       float4 val = *dst;
-      val.x += latent_noise(M, s, 0u, (uint32_t)e);
-      val.y += latent_noise(M, s, 0u, (uint32_t)(e + 1));
-      val.z += latent_noise(M, s, 0u, (uint32_t)(e + 2));
-      val.w += latent_noise(M, s, 0u, (uint32_t)(e + 3));
+      val.x += level_noise(L, 0u, (uint32_t)e);
+      val.y += level_noise(L, 0u, (uint32_t)(e + 1));
+      val.z += level_noise(L, 0u, (uint32_t)(e + 2));
+      val.w += level_noise(L, 0u, (uint32_t)(e + 3));
       *dst = val;
     }
   }
   {
     constexpr int C1 = SH::C1;
-    const int d1 = M.g1.dim[lvl];
+    const int d1 = L.d1;
     const int rowh = f1.w * (C1 / 2);
     float* foot1 = foot + f0.w * f0.h * SH::C0;
     for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
@@ -251,20 +290,70 @@ __device__ __forceinline__ void stage_noise(const Model& M, const StepRec& s, co
       const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
       float2* dst = reinterpret_cast<float2*>(foot1 + r * f1.w * C1 + q * 2);
       float2 val = *dst;
-      val.x += latent_noise(M, s, 1u, (uint32_t)e);
-      val.y += latent_noise(M, s, 1u, (uint32_t)(e + 1));
+      val.x += level_noise(L, 1u, (uint32_t)e);
+      val.y += level_noise(L, 1u, (uint32_t)(e + 1));
       *dst = val;
     }
   }
 }
 
-// Gathers half of one texel's feature row (draw_features arithmetic): half 0 the 4 C0 g0
-// corner features, half 1 the C1 bilinear g1 features, positional encoding, lod and padding.
-// `staged` reads the latents (noise already added) from the shared-memory boxes, otherwise
-// from global memory.
+// Buffered stores of a feature row half: 8 values per 16-byte chunk.
+struct RowWriter {
+  uint8_t* sX;
+  int row, col0, f;
+  float buf[8];
+};
+
+// Half of one texel's feature row (draw_features arithmetic, ntc_kernel.cu:75-177): half 0 the
+// 4 C0 g0 corner features, half 1 the C1 bilinear g1 features, positional encoding, lod and
+// padding.  `staged`: the latents (noise already added) come from the shared-memory boxes.
+// Otherwise gather_half_direct reads them, and adds the noise, from global memory.
 template <class SH>
-__device__ __forceinline__ void gather_half(const Model& M, const StepRec& s, int x, int y, bool valid, int row,
-                                           int half, bool staged, const Foot& f0, const Foot& f1, const float* foot,
+__device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int row, int half, uint8_t* sX)
+{
+  constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
+  constexpr int kSplit = 4 * C0;
+  const int col0 = half ? kSplit : 0;
+  Gather G;
+  gather_geometry(x, y, L.mip_dim, L.d0, L.d1, G);
+  float buf[8];
+  int f = 0;
+  auto put = [&](float v) {
+    buf[f & 7] = v;
+    f++;
+    if ((f & 7) == 0) st_chunk(sX, row, col0 + f - 8, Kp, buf);
+  };
+  if (half == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int base = G.c0[k] * C0;
+#pragma unroll
+      for (int c = 0; c < C0; c++) put(L.p0[base + c] + level_noise(L, 0u, (uint32_t)(base + c)));
+    }
+    return;
+  }
+  float acc[C1];
+#pragma unroll
+  for (int c = 0; c < C1; c++) acc[c] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int base = G.c1[k] * C1;
+#pragma unroll
+    for (int c = 0; c < C1; c++)
+      acc[c] = __fmaf_rn(G.w1[k], L.p1[base + c] + level_noise(L, 1u, (uint32_t)(base + c)), acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < C1; c++) put(acc[c]);
+#pragma unroll
+  for (int i = 0; i < 12; i++) put(pos_enc(x, y, i));
+  put(L.norm_lod);
+#pragma unroll
+  for (int i = 4 * C0 + C1 + 13; i < Kp; i++) put(0.0f);
+}
+
+template <class SH>
+__device__ __forceinline__ void gather_half(const LevelArgs& L, int x, int y, bool valid, int row, int half,
+                                           bool staged, const Foot& f0, const Foot& f1, const float* foot,
                                            uint8_t* sX)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
@@ -276,11 +365,14 @@ __device__ __forceinline__ void gather_half(const Model& M, const StepRec& s, in
     for (int c = col0; c < col1; c += 8) st_chunk(sX, row, c, Kp, z);
     return;
   }
-  const int lvl = s.level;
-  const int d0 = M.g0.dim[lvl], d1 = M.g1.dim[lvl];
+  if (!staged) {
+    gather_half_direct<SH>(L, x, y, row, half, sX);
+    return;
+  }
+  const int d0 = L.d0, d1 = L.d1;
   const int l0 = log2_pow2(d0), l1 = log2_pow2(d1);
   Gather G;
-  gather_geometry(x, y, s.mip_dim, d0, d1, G);
+  gather_geometry(x, y, L.mip_dim, d0, d1, G);
   float buf[8];
   int f = 0;  // features put so far (compile-time after unrolling, so buf stays in registers)
   auto put = [&](float v) {
@@ -291,30 +383,15 @@ __device__ __forceinline__ void gather_half(const Model& M, const StepRec& s, in
   if (half == 0) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      if (staged) {
-        const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
-        const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
+      const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
+      const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
 #pragma unroll
-        for (int c = 0; c < C0; c += 4) {
-          const float4 q = *reinterpret_cast<const float4*>(src + c);
-          put(q.x);
-          put(q.y);
-          put(q.z);
-          put(q.w);
-        }
-      } else {
-        const int base = G.c0[k] * C0;
-        const float* p0 = M.g0.p[lvl];
-#pragma unroll
-        for (int c = 0; c < C0; c += 4) {
-          const float4 q = *reinterpret_cast<const float4*>(p0 + base + c);
-          float v[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            if (s.noise) v[i] = v[i] + latent_noise(M, s, 0u, (uint32_t)(base + c + i));
-            put(v[i]);
-          }
-        }
+      for (int c = 0; c < C0; c += 4) {
+        const float4 q = *reinterpret_cast<const float4*>(src + c);
+        put(q.x);
+        put(q.y);
+        put(q.z);
+        put(q.w);
       }
     }
     return;
@@ -325,38 +402,43 @@ __device__ __forceinline__ void gather_half(const Model& M, const StepRec& s, in
   const float* foot1 = foot + f0.w * f0.h * C0;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    if (staged) {
-      const int cy = G.c1[k] >> l1, cx = G.c1[k] & (d1 - 1);
-      const float* src = foot1 + ((cy - f1.y0) * f1.w + (cx - f1.x0)) * C1;
+    const int cy = G.c1[k] >> l1, cx = G.c1[k] & (d1 - 1);
+    const float* src = foot1 + ((cy - f1.y0) * f1.w + (cx - f1.x0)) * C1;
 #pragma unroll
-      for (int c = 0; c < C1; c += 2) {
-        const float2 q = *reinterpret_cast<const float2*>(src + c);
-        acc[c] = __fmaf_rn(G.w1[k], q.x, acc[c]);
-        acc[c + 1] = __fmaf_rn(G.w1[k], q.y, acc[c + 1]);
-      }
-    } else {
-      const int base = G.c1[k] * C1;
-      const float* p1 = M.g1.p[lvl];
-#pragma unroll
-      for (int c = 0; c < C1; c += 2) {
-        const float2 q = *reinterpret_cast<const float2*>(p1 + base + c);
-        float a = q.x, b = q.y;
-        if (s.noise) {
-          a = a + latent_noise(M, s, 1u, (uint32_t)(base + c));
-          b = b + latent_noise(M, s, 1u, (uint32_t)(base + c + 1));
-        }
-        acc[c] = __fmaf_rn(G.w1[k], a, acc[c]);
-        acc[c + 1] = __fmaf_rn(G.w1[k], b, acc[c + 1]);
-      }
+    for (int c = 0; c < C1; c += 2) {
+      const float2 q = *reinterpret_cast<const float2*>(src + c);
+      acc[c] = __fmaf_rn(G.w1[k], q.x, acc[c]);
+      acc[c + 1] = __fmaf_rn(G.w1[k], q.y, acc[c + 1]);
     }
   }
 #pragma unroll
   for (int c = 0; c < C1; c++) put(acc[c]);
 #pragma unroll
   for (int i = 0; i < 12; i++) put(pos_enc(x, y, i));
-  put(s.norm_lod);
+  put(L.norm_lod);
 #pragma unroll
   for (int i = 4 * C0 + C1 + 13; i < Kp; i++) put(0.0f);
+}
+
+// Direct per-texel scatter of one row half (wrapped blocks, tiny tiles, oversized boxes):
+// half 0 the g0 corners, half 1 the bilinear g1 corners (ntc_kernel.cu:280-341).
+template <class SH>
+__device__ __noinline__ void scatter_direct(LevelArgs L, int x, int y, int half, const float* dxr)
+{
+  constexpr int C0 = SH::C0, C1 = SH::C1;
+  Gather G;
+  gather_geometry(x, y, L.mip_dim, L.d0, L.d1, G);
+  if (half == 0) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+      for (int c = 0; c < C0; c++) atomicAdd(&L.g0[G.c0[kk] * C0 + c], dxr[kk * C0 + c]);
+  } else {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+      for (int c = 0; c < C1; c++) atomicAdd(&L.g1[G.c1[kk] * C1 + c], G.w1[kk] * dxr[4 * C0 + c]);
+  }
 }
 
 // Loads the fp32 master weights into the bf16 canonical tiles (zero padding past F / C).
@@ -422,6 +504,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   __shared__ float u8_to_unit[256];  // v / 255 as upstream computes it (libopenntc draw_targets)
   __shared__ CornerMasks masks_s[2];
   __shared__ StepRec step_s;
+  __shared__ LevelArgs level_s;
 
   // The step record lives in shared memory: every group barrier (a memory clobber) makes the
   // compiler re-read the fields it uses, and there that costs a shared load, not an L1/L2 trip.
@@ -463,6 +546,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   ptx::fence_before_sync();
   __syncthreads();
   ptx::fence_after_sync();
+  if (tid == 0) level_s = level_args(M, s);  // published by the __syncthreads below
+  const LevelArgs& L = level_s;
   const uint32_t tbase = tmem_base_s;
   const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
   // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16): each of
@@ -518,8 +603,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   int pb = 0;
   {
     const int u0 = blockIdx.x * 2 + g;
-    nstaged = u0 < ntiles && unit_footprint<SH>(M, s, u0, nf0, nf1);
-    if (nstaged) stage_copy<SH>(M, s, nf0, nf1, gp.foot, gt);
+    nstaged = u0 < ntiles && unit_footprint<SH>(L, s, u0, nf0, nf1);
+    if (nstaged) stage_copy<SH>(L, nf0, nf1, gp.foot, gt);
     ptx::cp_async_commit();
   }
 
@@ -547,15 +632,15 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       // start the next unit's copy into the other buffer (its last reader, the gather of
       // the unit before this one, finished several group barriers ago)
       const int nu = unit + ustride;
-      nstaged = nu < ntiles && unit_footprint<SH>(M, s, nu, nf0, nf1);
-      if (nstaged) stage_copy<SH>(M, s, nf0, nf1, gp.foot + (pb ^ 1) * kFootBuf, gt);
+      nstaged = nu < ntiles && unit_footprint<SH>(L, s, nu, nf0, nf1);
+      if (nstaged) stage_copy<SH>(L, nf0, nf1, gp.foot + (pb ^ 1) * kFootBuf, gt);
       ptx::cp_async_commit();
       pb ^= 1;
     }
     CornerMasks& cm = masks_s[g];
     if (staged) {
       ptx::cp_async_wait<1>();  // this unit's copies (all but the group just committed)
-      if (s.noise) stage_noise<SH>(M, s, f0, f1, foot, gt);
+      if (s.noise) stage_noise<SH>(L, f0, f1, foot, gt);
       for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) {
         uint32_t* m = i < 2 * kMaxBoxW ? &cm.xlo[0][0] + i
                       : i < 4 * kMaxBoxW ? &cm.xhi[0][0] + (i - 2 * kMaxBoxW)
@@ -564,9 +649,9 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         *m = 0u;
       }
       bar_group(g);
-      build_masks(s, M.g0.dim[s.level], M.g1.dim[s.level], f0, f1, unit, cm, gt);
+      build_masks(s, L.d0, L.d1, f0, f1, unit, cm, gt);
     }
-    gather_half<SH>(M, s, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
+    gather_half<SH>(L, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -716,8 +801,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
     // ------------------------------------------------------------------ scatter dX
     if (s.grid_update) {
-      const int lvl = s.level;
-      const int d0 = M.g0.dim[lvl], d1 = M.g1.dim[lvl];
+      const int d0 = L.d0, d1 = L.d1;
       // dX rows to shared memory (the group's operand tiles are free now), half a row per thread
       constexpr int LD = Kp + 4;
       float* dxs = reinterpret_cast<float*>(gp.X);
@@ -731,8 +815,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
           *reinterpret_cast<float4*>(dxs + row * LD + half * KH + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);
       }
       bar_group(g);
-      float* g0p = M.g0.g[lvl];
-      float* g1p = M.g1.g[lvl];
+      float* g0p = L.g0;
+      float* g1p = L.g1;
       if (staged) {
         // owner-computes: a work item is one box cell and a group of its channels (4 of g0,
         // 2 of g1); its thread sums every texel-corner contribution to them
@@ -796,22 +880,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
           }
         }
       } else if (valid) {
-        // direct per-texel scatter (wrapped blocks, tiny tiles, oversized boxes): half 0 the
-        // g0 corners, half 1 the bilinear g1 corners of the row
-        Gather G;
-        gather_geometry(x, y, s.mip_dim, d0, d1, G);
-        const float* dxr = dxs + row * LD;
-        if (half == 0) {
-#pragma unroll
-          for (int kk = 0; kk < 4; kk++)
-#pragma unroll
-            for (int c = 0; c < C0; c++) atomicAdd(&g0p[G.c0[kk] * C0 + c], dxr[kk * C0 + c]);
-        } else {
-#pragma unroll
-          for (int kk = 0; kk < 4; kk++)
-#pragma unroll
-            for (int c = 0; c < C1; c++) atomicAdd(&g1p[G.c1[kk] * C1 + c], G.w1[kk] * dxr[4 * C0 + c]);
-        }
+        scatter_direct<SH>(L, x, y, half, dxs + row * LD);
       }
     }
     ptx::fence_before_sync();

@@ -51,9 +51,12 @@ def test_deferred_matches_dense(materials, precision):
     psnr_d, d, cd = _run(manifest, ont.LatentAdam.DEFERRED, precision, 150)
     print(f"PSNR dense {psnr_a:.4f} / {psnr_b:.4f}, deferred {psnr_d:.4f} dB")
     assert abs(psnr_d - psnr_a) < max(4 * abs(psnr_b - psnr_a), 0.02)
+    # Float atomics make every run differ slightly, most on small levels trained with whole-mip
+    # tiles; a missed or doubled replay would move a moment by a factor of beta^k, i.e. by
+    # tens of percent, far beyond this bound.
     for key in a:
         spread = np.abs(b[key] - a[key]).max()
         diff = np.abs(d[key] - a[key]).max()
         scale = np.abs(a[key]).max()
-        assert diff <= max(4 * spread, 1e-3 * scale), (key, diff, spread, scale)
+        assert diff <= max(8 * spread, 5e-3 * scale), (key, diff, spread, scale)
     del ca, cb, cd
