@@ -219,6 +219,17 @@ def fill_constants(data: CompressedData) -> Constants:
     return c
 
 
+def train_batch(contexts: list, num_batches: int) -> tuple[Result, list]:
+    """Advances every context by up to num_batches steps, overlapping their GPU work
+    (ontc_train_batch).  Returns the overall result and each context's TrainProgress."""
+    lib = load()
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.handle for c in contexts])
+    out = (TrainProgress * n)()
+    r = lib.ontc_train_batch(hs, n, int(num_batches), out)
+    return Result(r), list(out)
+
+
 class Decoder:
     """Batch SampleMaterial (ntc_decode.hlsli:605-623) of one compressed material on the GPU."""
 
