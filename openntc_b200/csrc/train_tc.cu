@@ -844,11 +844,11 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
                 }
               }
             }
+            // one 16-byte vector reduction per item (C0 % 4 == 0, latent buffers 256-byte aligned);
+            // adding +0 leaves a gradient unchanged, so a group with some zero sums adds them too
             float* dst = g0p + ((f0.y0 + by) * d0 + f0.x0 + bx) * C0 + 4 * q;
-            if (sum.x != 0.0f) atomicAdd(dst, sum.x);
-            if (sum.y != 0.0f) atomicAdd(dst + 1, sum.y);
-            if (sum.z != 0.0f) atomicAdd(dst + 2, sum.z);
-            if (sum.w != 0.0f) atomicAdd(dst + 3, sum.w);
+            if (sum.x != 0.0f || sum.y != 0.0f || sum.z != 0.0f || sum.w != 0.0f)
+              atomicAdd(reinterpret_cast<float4*>(dst), sum);
           } else {
             const int j = i - ni0;
             const int cell = j / Q1, q = j - cell * Q1;
@@ -875,8 +875,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
               }
             }
             float* dst = g1p + ((f1.y0 + by) * d1 + f1.x0 + bx) * C1 + 2 * q;
-            if (sum.x != 0.0f) atomicAdd(dst, sum.x);
-            if (sum.y != 0.0f) atomicAdd(dst + 1, sum.y);
+            if (sum.x != 0.0f || sum.y != 0.0f) atomicAdd(reinterpret_cast<float2*>(dst), sum);
           }
         }
       } else if (valid) {
