@@ -263,7 +263,7 @@ def run_ours(args):
             "metric": METRIC, "value": round(value, 1), "unit": "samples/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.precision,
-            "data": "synthetic: seeded 2048^2 9-channel PBR set (value-noise height, ramp albedo, normals, "
+            "data": f"synthetic: seeded {WORKLOAD['dim']}^2 9-channel PBR set (value-noise height, ramp albedo, normals, "
                     "roughness, metallic, AO), one material per rank",
             "config": dict(WORKLOAD, precision=args.precision, latent_adam=args.latent_adam, l2=L2_NOTE,
                            parallelism=f"replicas x{world} (independent materials, no collective)"),
@@ -427,7 +427,7 @@ def run_reference(args):
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "samples/s", "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32 (cuBLAS TF32 GEMMs)", "data": "synthetic: same seeded 2048^2 9-channel PBR set",
+        "dtype": "fp32 (cuBLAS TF32 GEMMs)", "data": f"synthetic: same seeded {WORKLOAD['dim']}^2 9-channel PBR set",
         "config": dict(WORKLOAD, precision="upstream"), "impl": "reference",
         "cpu_baseline": {"value": round(value, 1), "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
                          "sample": f"upstream Context::Train built from its own sources (cuBLAS TF32 + its CUDA "
@@ -442,6 +442,7 @@ def run_reference(args):
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--dim", type=int, default=0, help="training material size (default 2048)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
@@ -454,6 +455,9 @@ def main():
     ap.add_argument("--decode-samples", type=int, default=0, help="samples per decode (default 66,355,200)")
     args = ap.parse_args()
     assert args.warmup >= 3
+    if args.dim and args.dim != WORKLOAD["dim"]:
+        WORKLOAD["dim"] = args.dim
+        WORKLOAD["workload"] = f"train_{args.dim}sq_9ch_bpp1_0_b262144"
     if args.workload == "decode":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "upstream decodes in HLSL only "
