@@ -31,13 +31,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
   return ok != 0;
 }
 
-// Bounded wait: returns false after `limit` polls (the caller records an error and bails out).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = (1u << 24))
+// try_wait with a suspend-time hint: the thread sleeps in hardware until the phase completes or
+// about `hint_ns` nanoseconds pass, instead of spinning through issue slots.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns)
 {
-  for (uint32_t i = 0; i < limit; i++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (i > 64) __nanosleep(32);
-  }
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false after `limit` suspended polls of up to ~100 us each (about two
+// seconds in all; the caller records an error and bails out).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = 20000)
+{
+  for (uint32_t i = 0; i < limit; i++)
+    if (mbar_try_wait_sleep(bar, parity, 100000u)) return true;
   return false;
 }
 
