@@ -82,6 +82,11 @@ int ontc_debug_shape(ontc_context* ctx, int32_t* out32);
  * Returns their count, or -1 when more than cap are needed. */
 int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap);
 
+/* The bounded wait of the tcgen05 kernels, exercised: one GPU thread waits `polls` (1..1000)
+ * suspended polls of up to ~100 us on a barrier nothing arrives at.  Returns ONTC_CUDA_FAILURE
+ * when the wait gave up and reported it (the expected outcome), ONTC_INVALID_STATE otherwise. */
+int ontc_debug_wait_timeout(int32_t polls);
+
 #ifdef __cplusplus
 }
 #endif

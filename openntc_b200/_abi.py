@@ -149,6 +149,7 @@ SIGNATURES = {
     "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
     "ontc_debug_disjoint_cover": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
     "ontc_lanczos_down_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ontc_debug_wait_timeout": (C.c_int, [C.c_int32]),
     "ontc_train_batch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TrainProgress)]),
     "ontc_decoder_create": (C.c_int, [C.POINTER(CompressedData), C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "ontc_decoder_destroy": (None, [P]),

@@ -1525,6 +1525,18 @@ int ontc_debug_package(ontc_context* c, int32_t mip, uint8_t* out)
   return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
 }
 
+int ontc_debug_wait_timeout(int32_t polls)
+{
+  if (polls < 1 || polls > 1000) return ONTC_INVALID_STATE;
+  DBuf<int> flag;
+  if (flag.alloc(1)) return ONTC_ALLOCATION_FAILURE;
+  int h = -1;
+  cudaError_t e = launch_wait_check((uint32_t)polls, flag.p, 0);
+  if (!e) e = cudaMemcpy(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e) return ONTC_CUDA_FAILURE;
+  return h == 1 ? ONTC_CUDA_FAILURE : ONTC_INVALID_STATE;  // the wait must have given up
+}
+
 int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap)
 {
   if (n < 0 || cap < 0 || (n > 0 && (!in || !out))) return -1;

@@ -28,6 +28,8 @@ struct DecodeArgs {
   int* err;             // set to 1 when a bounded wait gave up
 };
 cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
+// one thread waits `polls` suspended polls on a barrier nothing arrives at; *d_out = 1 when it gave up
+cudaError_t launch_wait_check(uint32_t polls, int* d_out, cudaStream_t stream);
 
 struct TileOut {
   float* dW_partial;     // [grid][nW] per-CTA decoder gradient partial sums (kTrain)

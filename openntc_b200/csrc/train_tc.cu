@@ -151,6 +151,27 @@ __device__ __forceinline__ float level_noise(const LevelArgs& L, uint32_t which,
   return 0.0f;
 }
 
+// hardgelu of 8 fp32 accumulator values, computed on packed bf16 pairs (the results feed the next
+// bf16 MMA, so they are bf16 either way), as one 16-byte chunk of activations:
+//   c = clamp(x, -1.5, 1.5);  hg = c * (c + 1.5) * (1/3) + max(x - 1.5, 0)
+// (the second term is x - 1.5 above the knee, where c = 1.5 and the first term is 1.5).
+__device__ __forceinline__ uint4 hg_chunk_bf16(const float* x)
+{
+  const __nv_bfloat162 lo = __floats2bfloat162_rn(-1.5f, -1.5f), hi = __floats2bfloat162_rn(1.5f, 1.5f);
+  const __nv_bfloat162 third = __floats2bfloat162_rn(1.0f / 3.0f, 1.0f / 3.0f);
+  const __nv_bfloat162 zero = __floats2bfloat162_rn(0.0f, 0.0f);
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+    const __nv_bfloat162 c = __hmin2(__hmax2(v, lo), hi);
+    const __nv_bfloat162 mid = __hmul2(__hmul2(c, __hadd2(c, hi)), third);
+    const __nv_bfloat162 r = __hadd2(mid, __hmax2(__hsub2(v, hi), zero));
+    w[i] = *reinterpret_cast<const uint32_t*>(&r);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 // ---- latent footprint of a unit ---------------------------------------------------------
 struct Foot {
   int x0, y0, w, h;
@@ -668,12 +689,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     ptx::ld16(lwin + hc + 16, h0 + 16);
     ptx::ld_wait();
 #pragma unroll
-    for (int c = 0; c < 32; c += 8) {
-      float a[8];
-#pragma unroll
-      for (int j = 0; j < 8; j++) a[j] = hg_fast(h0[c + j]);
-      st_chunk(gp.P0, row, hc + c, 64, a);
-    }
+    for (int c = 0; c < 32; c += 8)
+      *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(h0 + c);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -689,12 +706,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     ptx::ld16(lwin + hc + 16, h1 + 16);
     ptx::ld_wait();
 #pragma unroll
-    for (int c = 0; c < 32; c += 8) {
-      float a[8];
-#pragma unroll
-      for (int j = 0; j < 8; j++) a[j] = hg_fast(h1[c + j]);
-      st_chunk(gp.P1, row, hc + c, 64, a);
-    }
+    for (int c = 0; c < 32; c += 8)
+      *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(h1 + c);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();

@@ -291,3 +291,16 @@ def test_adam_step_matches_oracle(materials, oracle):
     oracle.adam(p[:nupd], mm[:nupd], vv[:nupd], dW[:nupd].astype(np.float32), s.lr_dec, s.b1, s.b2, 0, 0.0)
     assert rel_err(H.tensor(ctx, _abi.DBG_W)[:nupd] - W[:nupd], p[:nupd] - W[:nupd]) < 5e-3
     assert np.array_equal(H.tensor(ctx, _abi.DBG_W)[nupd:], W[nupd:])  # padded Wout rows never move
+
+
+def test_bounded_wait_gives_up_and_leaves_the_device_usable(lib, oracle):
+    """The tcgen05 kernels' mbarrier waits are bounded: a wait nothing completes gives up after
+    its polls and is reported as a failure, and the device keeps working afterwards."""
+    import time
+    t0 = time.perf_counter()
+    assert lib.ontc_debug_wait_timeout(5) == ont.Result.CudaFailure
+    assert time.perf_counter() - t0 < 5.0
+    assert lib.ontc_debug_wait_timeout(0) == ont.Result.InvalidState
+    w = np.zeros(12, np.float32)
+    assert lib.ontc_debug_lanczos_weights(w.ctypes.data_as(C.c_void_p)) == 0  # still usable
+    assert np.abs(w - oracle.lanczos_weights()).max() < 1e-6
