@@ -97,17 +97,6 @@ __device__ __forceinline__ void st_chunk(uint8_t* base, int r, int c0, int cols,
 
 __device__ __forceinline__ void bar_group(int g) { asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory"); }
 
-// hardgelu and its derivative for the bf16 path: the division by 3 becomes a multiply by
-// the fp32 reciprocal (the operands are bf16-rounded anyway).
-__device__ __forceinline__ float hg_fast(float x)
-{
-  return x < -1.5f ? 0.0f : (x < 1.5f ? x * (x + 1.5f) * (1.0f / 3.0f) : x);
-}
-__device__ __forceinline__ float hg_grad_fast(float x)
-{
-  return x < -1.5f ? 0.0f : (x < 1.5f ? (2.0f * x + 1.5f) * (1.0f / 3.0f) : 1.0f);
-}
-
 // The step's level as the tile kernel uses it: resolved once per CTA into shared memory (the
 // Model's per-level arrays are kernel parameters indexed by a runtime level), and passed by
 // value to the out-of-line paths.
@@ -155,7 +144,7 @@ __device__ __forceinline__ float level_noise(const LevelArgs& L, uint32_t which,
 // bf16 MMA, so they are bf16 either way), as one 16-byte chunk of activations:
 //   c = clamp(x, -1.5, 1.5);  hg = c * (c + 1.5) * (1/3) + max(x - 1.5, 0)
 // (the second term is x - 1.5 above the knee, where c = 1.5 and the first term is 1.5).
-__device__ __forceinline__ uint4 hg_chunk_bf16(const float* x)
+__device__ __forceinline__ uint4 hg_chunk_bf16(const float* x, uint32_t* pre)
 {
   const __nv_bfloat162 lo = __floats2bfloat162_rn(-1.5f, -1.5f), hi = __floats2bfloat162_rn(1.5f, 1.5f);
   const __nv_bfloat162 third = __floats2bfloat162_rn(1.0f / 3.0f, 1.0f / 3.0f);
@@ -164,9 +153,32 @@ __device__ __forceinline__ uint4 hg_chunk_bf16(const float* x)
 #pragma unroll
   for (int i = 0; i < 4; i++) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+    pre[i] = *reinterpret_cast<const uint32_t*>(&v);  // kept for the backward pass
     const __nv_bfloat162 c = __hmin2(__hmax2(v, lo), hi);
     const __nv_bfloat162 mid = __hmul2(__hmul2(c, __hadd2(c, hi)), third);
     const __nv_bfloat162 r = __hadd2(mid, __hmax2(__hsub2(v, hi), zero));
+    w[i] = *reinterpret_cast<const uint32_t*>(&r);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// dA * hardgelu'(h) for 8 columns on packed bf16 pairs (pre: the packed pre-activations of the
+// forward pass), as one 16-byte chunk:
+//   hg'(x) = x < -1.5 ? 0 : x < 1.5 ? (2x + 1.5) / 3 : 1
+//          = [x >= -1.5] * (c * 2/3 + 0.5 - 0.5 * [x >= 1.5]),  c = clamp(x, -1.5, 1.5)
+__device__ __forceinline__ uint4 dhg_chunk_bf16(const float* da, const uint32_t* pre)
+{
+  const __nv_bfloat162 lo = __floats2bfloat162_rn(-1.5f, -1.5f), hi = __floats2bfloat162_rn(1.5f, 1.5f);
+  const __nv_bfloat162 two3 = __floats2bfloat162_rn(2.0f / 3.0f, 2.0f / 3.0f);
+  const __nv_bfloat162 half = __floats2bfloat162_rn(0.5f, 0.5f), mhalf = __floats2bfloat162_rn(-0.5f, -0.5f);
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const __nv_bfloat162 x = *reinterpret_cast<const __nv_bfloat162*>(&pre[i]);
+    const __nv_bfloat162 c = __hmin2(__hmax2(x, lo), hi);
+    const __nv_bfloat162 d = __hfma2(__hge2(x, hi), mhalf, __hfma2(c, two3, half));
+    const __nv_bfloat162 gr = __hmul2(__hge2(x, lo), d);
+    const __nv_bfloat162 r = __hmul2(__floats2bfloat162_rn(da[2 * i], da[2 * i + 1]), gr);
     w[i] = *reinterpret_cast<const uint32_t*>(&r);
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
@@ -684,13 +696,14 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 0 epilogue
-    float h0[32], h1[32];
-    ptx::ld16(lwin + hc, h0);
-    ptx::ld16(lwin + hc + 16, h0 + 16);
+    uint32_t h0[16], h1[16];  // pre-activations of this thread's 32 columns, packed bf16 pairs
+    float hx[32];
+    ptx::ld16(lwin + hc, hx);
+    ptx::ld16(lwin + hc + 16, hx + 16);
     ptx::ld_wait();
 #pragma unroll
     for (int c = 0; c < 32; c += 8)
-      *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(h0 + c);
+      *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(hx + c, h0 + c / 2);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -702,12 +715,12 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 1 epilogue
-    ptx::ld16(lwin + hc, h1);
-    ptx::ld16(lwin + hc + 16, h1 + 16);
+    ptx::ld16(lwin + hc, hx);
+    ptx::ld16(lwin + hc + 16, hx + 16);
     ptx::ld_wait();
 #pragma unroll
     for (int c = 0; c < 32; c += 8)
-      *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(h1 + c);
+      *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(hx + c, h1 + c / 2);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -757,12 +770,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
 #pragma unroll
-      for (int c = 0; c < 32; c += 8) {
-        float gv[8];
-#pragma unroll
-        for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h1[c + j]);
-        st_chunk(gp.P1, row, hc + c, 64, gv);
-      }
+      for (int c = 0; c < 32; c += 8)
+        *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = dhg_chunk_bf16(da + c, h1 + c / 2);
     }
     handoff();
     if (issuer) {
@@ -788,12 +797,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
 #pragma unroll
-      for (int c = 0; c < 32; c += 8) {
-        float gv[8];
-#pragma unroll
-        for (int j = 0; j < 8; j++) gv[j] = da[c + j] * hg_grad_fast(h0[c + j]);
-        st_chunk(gp.P0, row, hc + c, 64, gv);
-      }
+      for (int c = 0; c < 32; c += 8)
+        *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = dhg_chunk_bf16(da + c, h0 + c / 2);
     }
     handoff();
     if (issuer) {
