@@ -973,141 +973,148 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
   int cnt = std::min(chunk_cap, target - first);
   // a chunk ends at the lock step so the latents can be snapped before it runs
   if (first < c->lock_i && first + cnt > c->lock_i) cnt = c->lock_i - first;
-  for (int k = 0; k < cnt; k++) {
-    const int bi = first + k;
-    const bool draw_uniform = dist_batch_type(c->gen);
-    const float U = dist_u(c->gen);
-    const float fl = std::floor(0.5f * -std::log2(U));
-    int lod = (fl < 1e9f) ? std::min((int)fl, c->mips - 1) : c->mips - 1;
-    const int lod_uniform = dist_lod(c->gen);
-    if (draw_uniform) lod = lod_uniform;
-    StepRec& s = c->h_steps[k];
-    s = StepRec();
-    s.lod = lod;
-    s.level = c->feature_level_for_lod(lod);
-    s.mip_dim = c->mip_dim[lod];
-    std::uniform_int_distribution<int> dist_grid(0, c->mip_dim[lod] - 1);
-    for (int g = 0; g < c->grids; g++) {
-      s.ox[g] = dist_grid(c->gen);
-      s.oy[g] = dist_grid(c->gen);
-    }
-    s.tile_dim = std::min(c->mip_dim[lod], 256);
-    s.n_grids = c->grids;
-    s.texels = c->grids * s.tile_dim * s.tile_dim;
-    s.noise = bi < c->lock_i ? (c->noise_mode == ONTC_NOISE_UPSTREAM ? 2 : 1) : 0;
-    s.grid_update = bi < c->lock_i ? 1 : 0;
-    s.seed = step_seed((uint32_t)bi);
-    s.norm_lod = lod / static_cast<float>(c->mips - 1);
-    s.b1 = 1.0f / (1.0f - powf(0.9f, bi + 1.0f));
-    s.b2 = 1.0f / (1.0f - powf(0.999f, bi + 1.0f));
-    s.gb1 = 1.0f / (1.0f - powf(0.9f, c->grid_batch_i[s.level] + 1.0f));
-    s.gb2 = 1.0f / (1.0f - powf(0.999f, c->grid_batch_i[s.level] + 1.0f));
-    c->grid_batch_i[s.level] += 1;
-    // deferred optimiser bookkeeping, in step order: the floor each level is swept to
-    s.gstep = c->upd_count[s.level];
-    s.gfloor = 0;
-    s.sweep_from = -1;
-    if (bi == c->lock_i && c->optimizer == ONTC_LATENT_ADAM_DEFERRED)
-      for (int l = 0; l < c->levels; l++) {
-        c->lock_from[l] = c->swept[l];
-        c->lock_to[l] = c->upd_count[l];
-        c->swept[l] = c->upd_count[l];
+  // Steps are drawn, uploaded and launched kPrepBatch at a time, so the GPU starts after the
+  // first few and the host prepares the rest while it runs (every step has its own staging slot).
+  constexpr int kPrepBatch = 8;
+  for (int k0 = 0; k0 < cnt && e == cudaSuccess; k0 += kPrepBatch) {
+    const int k1 = std::min(cnt, k0 + kPrepBatch);
+    for (int k = k0; k < k1; k++) {
+      const int bi = first + k;
+      const bool draw_uniform = dist_batch_type(c->gen);
+      const float U = dist_u(c->gen);
+      const float fl = std::floor(0.5f * -std::log2(U));
+      int lod = (fl < 1e9f) ? std::min((int)fl, c->mips - 1) : c->mips - 1;
+      const int lod_uniform = dist_lod(c->gen);
+      if (draw_uniform) lod = lod_uniform;
+      StepRec& s = c->h_steps[k];
+      s = StepRec();
+      s.lod = lod;
+      s.level = c->feature_level_for_lod(lod);
+      s.mip_dim = c->mip_dim[lod];
+      std::uniform_int_distribution<int> dist_grid(0, c->mip_dim[lod] - 1);
+      for (int g = 0; g < c->grids; g++) {
+        s.ox[g] = dist_grid(c->gen);
+        s.oy[g] = dist_grid(c->gen);
       }
-    if (s.grid_update) {
-      c->upd_count[s.level] += 1;
-      if (c->optimizer == ONTC_LATENT_ADAM_DEFERRED) {
-        // a cell may lag its level by at most kHistRing steps (the ring of step scalars); the
-        // level is swept every kSweepEvery level steps
-        if (s.gstep - c->swept[s.level] >= kSweepEvery) {
-          s.sweep_from = c->swept[s.level];
-          c->swept[s.level] = s.gstep;
+      s.tile_dim = std::min(c->mip_dim[lod], 256);
+      s.n_grids = c->grids;
+      s.texels = c->grids * s.tile_dim * s.tile_dim;
+      s.noise = bi < c->lock_i ? (c->noise_mode == ONTC_NOISE_UPSTREAM ? 2 : 1) : 0;
+      s.grid_update = bi < c->lock_i ? 1 : 0;
+      s.seed = step_seed((uint32_t)bi);
+      s.norm_lod = lod / static_cast<float>(c->mips - 1);
+      s.b1 = 1.0f / (1.0f - powf(0.9f, bi + 1.0f));
+      s.b2 = 1.0f / (1.0f - powf(0.999f, bi + 1.0f));
+      s.gb1 = 1.0f / (1.0f - powf(0.9f, c->grid_batch_i[s.level] + 1.0f));
+      s.gb2 = 1.0f / (1.0f - powf(0.999f, c->grid_batch_i[s.level] + 1.0f));
+      c->grid_batch_i[s.level] += 1;
+      // deferred optimiser bookkeeping, in step order: the floor each level is swept to
+      s.gstep = c->upd_count[s.level];
+      s.gfloor = 0;
+      s.sweep_from = -1;
+      if (bi == c->lock_i && c->optimizer == ONTC_LATENT_ADAM_DEFERRED)
+        for (int l = 0; l < c->levels; l++) {
+          c->lock_from[l] = c->swept[l];
+          c->lock_to[l] = c->upd_count[l];
+          c->swept[l] = c->upd_count[l];
         }
-        s.gfloor = c->swept[s.level];
-        make_foot(c, s, c->h_foots[k]);
+      if (s.grid_update) {
+        c->upd_count[s.level] += 1;
+        if (c->optimizer == ONTC_LATENT_ADAM_DEFERRED) {
+          // a cell may lag its level by at most kHistRing steps (the ring of step scalars); the
+          // level is swept every kSweepEvery level steps
+          if (s.gstep - c->swept[s.level] >= kSweepEvery) {
+            s.sweep_from = c->swept[s.level];
+            c->swept[s.level] = s.gstep;
+          }
+          s.gfloor = c->swept[s.level];
+          make_foot(c, s, c->h_foots[k]);
+        }
       }
+      s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
+      s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
+      s.step = bi;
     }
-    s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
-    s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
-    s.step = bi;
-  }
-  e = cudaMemcpyAsync(c->steps.p, c->h_steps, cnt * sizeof(StepRec), cudaMemcpyHostToDevice, c->stream);
-  for (int k = 0; k < cnt && e == cudaSuccess; k++) {
-    const int bi = first + k;
-    const StepRec& s = c->h_steps[k];
-    if (c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
-      // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
-      for (int g = 0; g < 2 && e == cudaSuccess; g++)
-        e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
-                              g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
-      c->launches += 2;
-    }
-    if (bi == c->lock_i) {
-      // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
-      if (!e && c->optimizer == ONTC_LATENT_ADAM_DEFERRED) e = sweep_levels(c, c->lock_from, c->lock_to);
-      for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
-        e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
-        if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
+    e = cudaMemcpyAsync(c->steps.p + k0, c->h_steps + k0, (k1 - k0) * sizeof(StepRec), cudaMemcpyHostToDevice,
+                        c->stream);
+    for (int k = k0; k < k1 && e == cudaSuccess; k++) {
+      const int bi = first + k;
+      const StepRec& s = c->h_steps[k];
+      if (c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
+        // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
+        for (int g = 0; g < 2 && e == cudaSuccess; g++)
+          e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
+                                g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
         c->launches += 2;
       }
-      for (int g = 0; g < 2 && e == cudaSuccess; g++)
-        if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
-    }
-    const bool deferred = c->optimizer == ONTC_LATENT_ADAM_DEFERRED && s.grid_update;
-    const FootRec& fr = c->h_foots[k];
-    if (deferred) {
-      if (s.sweep_from >= 0) {
+      if (bi == c->lock_i) {
+        // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
+        if (!e && c->optimizer == ONTC_LATENT_ADAM_DEFERRED) e = sweep_levels(c, c->lock_from, c->lock_to);
+        for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
+          e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
+          if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
+          c->launches += 2;
+        }
+        for (int g = 0; g < 2 && e == cudaSuccess; g++)
+          if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
+      }
+      const bool deferred = c->optimizer == ONTC_LATENT_ADAM_DEFERRED && s.grid_update;
+      const FootRec& fr = c->h_foots[k];
+      if (deferred) {
+        if (s.sweep_from >= 0) {
+          c->prof_begin();
+          if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
+          c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)),
+                      0.0);
+          c->launches++;
+        }
         c->prof_begin();
-        if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
-        c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)),
-                    0.0);
+        if (!e) e = launch_catchup(M, c->steps.p, k, fr, c->stream);
+        // reads and writes p, m, v of the footprint latents that lag
+        c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
         c->launches++;
       }
+      const int units = (s.texels + kTile - 1) / kTile;
+      TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
+      int grid = std::min(units, c->sms);
+      int cls = ONTC_KCLASS_UNITS_FP32;
       c->prof_begin();
-      if (!e) e = launch_catchup(M, c->steps.p, k, fr, c->stream);
-      // reads and writes p, m, v of the footprint latents that lag
-      c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
-      c->launches++;
-    }
-    const int units = (s.texels + kTile - 1) / kTile;
-    TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
-    int grid = std::min(units, c->sms);
-    int cls = ONTC_KCLASS_UNITS_FP32;
-    c->prof_begin();
-    if (c->precision == ONTC_PRECISION_BF16) {
-      grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
-      cls = ONTC_KCLASS_UNITS_BF16;
-      e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
-      if (e == cudaErrorNotSupported) {
-        cudaGetLastError();
-        grid = std::min(units, c->sms);
-        cls = ONTC_KCLASS_UNITS_FP32;
+      if (c->precision == ONTC_PRECISION_BF16) {
+        grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
+        cls = ONTC_KCLASS_UNITS_BF16;
+        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
+        if (e == cudaErrorNotSupported) {
+          cudaGetLastError();
+          grid = std::min(units, c->sms);
+          cls = ONTC_KCLASS_UNITS_FP32;
+          e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+        }
+      } else {
         e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
       }
-    } else {
-      e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+      // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
+      c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
+      c->launches++;
+      c->prof_begin();
+      if (deferred) {
+        if (!e)
+          e = launch_footprint_update(M, c->steps.p, k, fr, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
+                                      c->stream);
+        // footprint latents: p, m, v, g in and out (32 B each)
+        c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
+      } else {
+        if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
+        // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
+        c->prof_end(ONTC_KCLASS_ADAM,
+                    s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
+                    0.0);
+      }
+      c->launches++;
+      c->last_seed = s.seed;
+      c->last_noise = s.noise != 0;
+      c->last_step = s;
+      c->batch_i = bi + 1;
     }
-    // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
-    c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
-    c->launches++;
-    c->prof_begin();
-    if (deferred) {
-      if (!e)
-        e = launch_footprint_update(M, c->steps.p, k, fr, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
-                                    c->stream);
-      // footprint latents: p, m, v, g in and out (32 B each)
-      c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
-    } else {
-      if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
-      // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
-      c->prof_end(ONTC_KCLASS_ADAM,
-                  s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
-                  0.0);
-    }
-    c->launches++;
-    c->last_seed = s.seed;
-    c->last_noise = s.noise != 0;
-    c->last_step = s;
-    c->batch_i = bi + 1;
   }
   return e;
 }
