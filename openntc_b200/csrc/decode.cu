@@ -186,23 +186,31 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
     const float half = (float)(1u << (B1 - 1)), rhalf = 1.0f / half;
     const float mh[4] = {__fmul_rn(mult[0], rhalf), __fmul_rn(mult[1], rhalf), __fmul_rn(mult[2], rhalf),
                          __fmul_rn(mult[3], rhalf)};
-    float blend[C1];
+    static_assert(C1 % 2 == 0, "g1 channels blend in pairs");
+    float2 blend[C1 / 2];
 #pragma unroll
-    for (int c = 0; c < C1; c++) blend[c] = 0.0f;
+    for (int c = 0; c < C1 / 2; c++) blend[c] = make_float2(0.0f, 0.0f);
+    const float2 off = make_float2(-(8388608.0f + half), -(8388608.0f + half));
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int cx = clampi(hx + (q & 1), 0, d1 - 1), cy = clampi(hy + (q >> 1), 0, d1 - 1);
       uint32_t st[(C1 * B1 + 31) / 32];
       cell_stream<C1 * B1>(A.g1, A.g1_words, o1, (uint32_t)(cy * d1 + cx), st);
+      const float2 m2 = make_float2(mh[q], mh[q]);
 #pragma unroll
-      for (int c = 0; c < C1; c++) {
-        const uint32_t code = code_of<B1>(st, c);
-        const float centred = __fsub_rn(__uint_as_float(0x4B000000u | code), 8388608.0f + half);  // code - half
-        blend[c] = __fmaf_rn(mh[q], centred, blend[c]);
+      for (int c = 0; c < C1; c += 2) {
+        // code - half, exactly, for two channels; then the weighted blend on the pair
+        const float2 centred = ptx::add2(make_float2(__uint_as_float(0x4B000000u | code_of<B1>(st, c)),
+                                                     __uint_as_float(0x4B000000u | code_of<B1>(st, c + 1))),
+                                         off);
+        blend[c / 2] = ptx::fma2(m2, centred, blend[c / 2]);
       }
     }
 #pragma unroll
-    for (int c = 0; c < C1; c++) put_byte(w, 4 * C0 + c, q8(__fmul_rn(blend[c], 128.0f)));
+    for (int c = 0; c < C1; c += 2) {
+      put_byte(w, 4 * C0 + c, q8(__fmul_rn(blend[c / 2].x, 128.0f)));
+      put_byte(w, 4 * C0 + c + 1, q8(__fmul_rn(blend[c / 2].y, 128.0f)));
+    }
   }
   // 12 triangle waves of the texel coordinate at this lod, then the normalised lod
   {
@@ -233,17 +241,32 @@ __device__ __forceinline__ void st16(uint8_t* base, int r, int c0, int cols, uin
   *reinterpret_cast<uint4*>(base + ptx::cm_off8(r, c0, cols)) = make_uint4(a, b, c, d);
 }
 
-// 16 accumulator columns of this thread's row -> 16 requantised activations (4 words).
+// 16 accumulator columns of this thread's row -> 16 requantised activations (4 words).  The
+// arithmetic of hg_hlsl and q8_bits, two columns at a time on packed fp32 pairs (each lane
+// rounds exactly as the scalar operation).
 __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restrict__ scale, float rcp, uint32_t* out)
 {
   float acc[16];
   ptx::ld16(taddr, acc);
   ptx::ld_wait();
+  const float2 third = make_float2(1.0f / 3.0f, 1.0f / 3.0f), m3 = make_float2(-3.0f, -3.0f);
+  const float2 h15 = make_float2(1.5f, 1.5f), r2 = make_float2(rcp, rcp);
+  const float2 magic = make_float2(12582912.0f, 12582912.0f);
   uint32_t b[16];
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
-    const float x = __fmul_rn((float)__float_as_int(acc[j]), scale[j]);
-    b[j] = q8_bits(__fmul_rn(hg_hlsl(x), rcp));
+  for (int j = 0; j < 16; j += 2) {
+    const float2 x = ptx::mul2(make_float2((float)__float_as_int(acc[j]), (float)__float_as_int(acc[j + 1])),
+                               *reinterpret_cast<const float2*>(scale + j));
+    const float2 c = make_float2(fmaxf(x.x, -1.5f), fmaxf(x.y, -1.5f));
+    const float2 q = ptx::mul2(c, third);                    // div3: RN(c * RN(1/3)),
+    const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);  // corrected by the exact remainder
+    const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
+    const float2 hg = make_float2(x.x < 1.5f ? mid.x : x.x, x.y < 1.5f ? mid.y : x.y);
+    float2 f = ptx::mul2(hg, r2);
+    f = make_float2(fminf(fmaxf(f.x, -128.0f), 127.0f), fminf(fmaxf(f.y, -128.0f), 127.0f));
+    const float2 k = ptx::add2(f, magic);
+    b[j] = __float_as_uint(k.x);
+    b[j + 1] = __float_as_uint(k.y);
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) out[i] = pack4(b[4 * i], b[4 * i + 1], b[4 * i + 2], b[4 * i + 3]);
@@ -281,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   __shared__ __align__(8) uint64_t bars[kGroups];
   __shared__ uint32_t tmem_base_s;
   __shared__ int fail_s;
-  __shared__ float s0[kHid], s1[kHid], so[kOutRows];
+  __shared__ __align__(16) float s0[kHid], s1[kHid], so[kOutRows];  // read as float2 pairs
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
