@@ -266,6 +266,61 @@ int ontc_decode_host(ontc_decoder* dec, const float* uv, const int32_t* lod, int
 /* Waits for the decoder's stream; ONTC_CUDA_FAILURE if a decode failed or timed out. */
 int ontc_decoder_status(ontc_decoder* dec);
 
+/* MaterialParams (ntc_decode.hlsli:507-522), 72 bytes, filled as DecodeMaterial (:544-603)
+ * does: every field starts at DefaultMaterialParams (:524-540) (albedo 0.5, alpha 1,
+ * displacement 0.5, emissive 0, gloss 0, metallic 0, normal (0.5, 0.5, 1), ao 1, roughness 1,
+ * specular 0.5, transmission 0); channel i < channel_count writes its saturated output into
+ * the field of its semantic (the k-th channel of a run of equal semantics into component k of
+ * a vector field; components past the third, undefined in the HLSL, are dropped, as are
+ * channels of semantic None), and `present`
+ * gets bit (1 << semantic) for every such channel. */
+typedef struct ontc_material_params {
+  float albedo[3];
+  float alpha;
+  float displacement;
+  float emissive;
+  float gloss;
+  float metallic;
+  float normal[3];
+  float ao;
+  float roughness;
+  float specular[3];
+  float transmission;
+  uint32_t present;
+} ontc_material_params;
+
+/* SampleMaterial with its DecodeMaterial step (ntc_decode.hlsli:605-623): n samples from DEVICE
+ * buffers d_uv [n][2], d_lod [n] into d_params [n].  Enqueued on the decoder's stream. */
+int ontc_decode_material(ontc_decoder* dec, const float* d_uv, const int32_t* d_lod, int64_t n,
+                         ontc_material_params* d_params);
+
+/* Flags of ontc_sample_screen. */
+enum {
+  ONTC_SCREEN_DISCARD_OUTSIDE = 1, /* pixels whose uv has a component outside [0, 1] are left
+                                      unwritten (flat_ntc.hlsl:76-77) */
+  ONTC_SCREEN_MATERIAL = 2         /* d_out is ontc_material_params [height][width] instead of
+                                      f32 [height][width][channel_count] */
+};
+
+/* Screen-space sampling, the NTC pixel shaders' sampling (flat_ntc.hlsl:78-84,
+ * pbr_ntc.hlsl:96-104) over a uv image: d_uv [height][width][2] f32 holds each pixel's
+ * interpolated uv (unjittered, row 0 at the top).  Per pixel:
+ *   - ComputeLod (ntc_decode.hlsli:152-168): ddx/ddy of uv as HLSL's ddx/ddy (coarse
+ *     derivatives): over the pixel's 2x2 quad, ddx = uv(x0+1, y0) - uv(x0, y0) and
+ *     ddy = uv(x0, y0+1) - uv(x0, y0) with (x0, y0) the quad's top-left pixel; where the quad
+ *     is cut by an odd width or height the missing neighbour is replaced by the backward
+ *     difference (uv(x0, y0) - uv(x0-1, y0)), and by 0 in a 1-pixel dimension;
+ *   - noise position = pixel centre (x + 0.5, y + 0.5) + 5.588238 * noise_frame
+ *     (flat_ntc.hlsl:82);
+ *   - StochasticFilterLod and StochasticFilterUv (:172-185) with InterleavedGradientNoise
+ *     (:143-146), then SampleMaterial at the jittered uv and the chosen lod.
+ * Every float step is one IEEE round-to-nearest operation in the order written in the HLSL
+ * (no fused multiply-add); log2 is CUDA's log2f (within 1 ulp), so the lod of a pixel whose
+ * noise value lies within a few ulps of the lod's fraction may differ from an exactly rounded
+ * log2 by one.  flags: ONTC_SCREEN_*.  Enqueued on the decoder's stream. */
+int ontc_sample_screen(ontc_decoder* dec, const float* d_uv, int32_t width, int32_t height, float noise_frame,
+                       int32_t flags, void* d_out);
+
 /* ---- Library facts and kernel timing (no upstream counterpart) ------------------------- */
 
 /* Number of kernel launches this context issued so far (all of them are libontc's own). */

@@ -233,6 +233,9 @@ def train_batch(contexts: list, num_batches: int) -> tuple[Result, list]:
 class Decoder:
     """Batch SampleMaterial (ntc_decode.hlsli:605-623) of one compressed material on the GPU."""
 
+    DISCARD_OUTSIDE = _abi.SCREEN_DISCARD_OUTSIDE  # sample_screen flags
+    MATERIAL = _abi.SCREEN_MATERIAL
+
     def __init__(self, data: CompressedData, stream: int | None = None):
         self._lib = load()
         h = C.c_void_p()
@@ -268,6 +271,15 @@ class Decoder:
 
     def status(self) -> Result:
         return Result(self._lib.ontc_decoder_status(self._h))
+
+    def decode_material(self, d_uv: int, d_lod: int, n: int, d_params: int) -> Result:
+        """SampleMaterial with DecodeMaterial: d_params is ontc_material_params [n] (18 words each)."""
+        return Result(self._lib.ontc_decode_material(self._h, d_uv, d_lod, n, d_params))
+
+    def sample_screen(self, d_uv: int, width: int, height: int, noise_frame: float, flags: int, d_out: int) -> Result:
+        """Stochastic screen-space sampling of a [height][width][2] uv image (device pointers);
+        flags: SCREEN_DISCARD_OUTSIDE | SCREEN_MATERIAL."""
+        return Result(self._lib.ontc_sample_screen(self._h, d_uv, width, height, noise_frame, flags, d_out))
 
 
 def semantic_from_name(name: str) -> int:

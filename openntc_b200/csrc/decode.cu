@@ -294,6 +294,83 @@ __device__ void load_decoder(const uint8_t* __restrict__ blob, uint8_t* W0, uint
   for (int i = threadIdx.x; i < kOutRows; i += kThreads) so[i] = sc[2 * kHid + i];
 }
 
+// InterleavedGradientNoise (ntc_decode.hlsli:143-146), each operation rounded on its own.
+__device__ __forceinline__ float ign(float x, float y)
+{
+  const float t = __fadd_rn(__fmul_rn(0.06711056f, x), __fmul_rn(0.00583715f, y));
+  const float r = __fmul_rn(52.9829189f, __fsub_rn(t, floorf(t)));
+  return __fsub_rn(r, floorf(r));
+}
+
+// HLSL's coarse ddx (axis 0) or ddy (axis 1) of the uv image at the quad whose top-left pixel
+// is `c0` = (x0, y0): the forward difference along the quad's first row / column, the backward
+// one where the image ends inside the quad, 0 in a one-pixel dimension.
+__device__ __forceinline__ float2 quad_delta(const float2* __restrict__ img, int64_t c0, float2 c, int64_t pos,
+                                             int64_t extent, int64_t step)
+{
+  if (pos + 1 < extent) {
+    const float2 n = img[c0 + step];
+    return make_float2(__fsub_rn(n.x, c.x), __fsub_rn(n.y, c.y));
+  }
+  if (pos > 0) {
+    const float2 n = img[c0 - step];
+    return make_float2(__fsub_rn(c.x, n.x), __fsub_rn(c.y, n.y));
+  }
+  return make_float2(0.0f, 0.0f);
+}
+
+// The NTC pixel shaders' stochastic filter (flat_ntc.hlsl:78-84) for pixel i of the uv image:
+// ComputeLod (ntc_decode.hlsli:152-168), StochasticFilterLod (:172-177), StochasticFilterUv
+// (:181-185).  Returns false for a pixel the shader discards (flat_ntc.hlsl:76-77).
+__device__ __forceinline__ bool screen_sample(const DecodeArgs& A, int64_t i, float& u, float& v, int& lod)
+{
+  const int64_t W = A.screen_w, H = A.screen_h;
+  const int64_t y = i / W, x = i - y * W;
+  const float2* __restrict__ img = reinterpret_cast<const float2*>(A.uv);
+  const float2 p = img[i];
+  const int64_t x0 = x & ~1ll, y0 = y & ~1ll, c0 = y0 * W + x0;
+  const float2 c = img[c0];
+  const float dim = (float)A.k.dim;
+  const float2 dx = quad_delta(img, c0, c, x0, W, 1), dy = quad_delta(img, c0, c, y0, H, W);
+  const float2 du = make_float2(__fmul_rn(dx.x, dim), __fmul_rn(dx.y, dim));
+  const float2 dv = make_float2(__fmul_rn(dy.x, dim), __fmul_rn(dy.y, dim));
+  const float gu = __fadd_rn(__fmul_rn(du.x, du.x), __fmul_rn(du.y, du.y));
+  const float gv = __fadd_rn(__fmul_rn(dv.x, dv.x), __fmul_rn(dv.y, dv.y));
+  const float2 major_d = gu > gv ? du : dv;
+  const float2 foot = make_float2(__fdiv_rn(major_d.x, dim), __fdiv_rn(major_d.y, dim));
+  const float major = __fsqrt_rn(fmaxf(gu, gv));
+  const float minor = fmaxf(__fsqrt_rn(fminf(gu, gv)), __fdiv_rn(major, 8.0f));  // max_aniso 8
+  const float lodab = fminf(fmaxf(log2f(minor), 0.0f), (float)(A.k.mip_count - 1));
+  // noise position: pixel centre + 5.588238 * noise_frame
+  const float nf = __fmul_rn(5.588238f, A.noise_frame);
+  const float px = __fadd_rn(__fadd_rn((float)x, 0.5f), nf), py = __fadd_rn(__fadd_rn((float)y, 0.5f), nf);
+  lod = (int)lodab + (ign(px, py) < __fsub_rn(lodab, floorf(lodab)) ? 1 : 0);
+  const float jitter = __fsub_rn(ign(__fadd_rn(px, 61.0f), __fadd_rn(py, 37.0f)), 0.5f);
+  u = __fadd_rn(p.x, __fmul_rn(foot.x, jitter));
+  v = __fadd_rn(p.y, __fmul_rn(foot.y, jitter));
+  return !(A.discard_outside && (p.x < 0.0f || p.y < 0.0f || p.x > 1.0f || p.y > 1.0f));
+}
+
+// DefaultMaterialParams (ntc_decode.hlsli:524-540) in ontc_material_params order.
+__device__ __forceinline__ void store_material(float* o, const float* y, int C, const DecodeArgs& A)
+{
+  float2* o2 = reinterpret_cast<float2*>(o);  // records are 72 bytes: 8-byte aligned
+  o2[0] = make_float2(0.5f, 0.5f);                        // albedo
+  o2[1] = make_float2(0.5f, 1.0f);                        // albedo.z, alpha
+  o2[2] = make_float2(0.5f, 0.0f);                        // displacement, emissive
+  o2[3] = make_float2(0.0f, 0.0f);                        // gloss, metallic
+  o2[4] = make_float2(0.5f, 0.5f);                        // normal.xy
+  o2[5] = make_float2(1.0f, 1.0f);                        // normal.z, ao
+  o2[6] = make_float2(1.0f, 0.5f);                        // roughness, specular.x
+  o2[7] = make_float2(0.5f, 0.5f);                        // specular.yz
+  o2[8] = make_float2(0.0f, __uint_as_float(A.material_present));  // transmission, present
+  // DecodeMaterial (:544-603): channel c into its field; a later channel of the same scalar
+  // field overwrites an earlier one (same thread, program order)
+#pragma unroll
+  for (int c = 0; c < kOutRows; c++)
+    if (c < C && A.material_dst[c] >= 0) o[A.material_dst[c]] = y[c];
+}
+
 template <class SH>
 __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_constant__ DecodeArgs A)
 {
@@ -357,13 +434,22 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   const int64_t ntiles = (A.n + 127) / 128;
   for (int64_t t = (int64_t)blockIdx.x * kGroups + g; t < ntiles; t += (int64_t)gridDim.x * kGroups) {
     const int64_t i = t * 128 + row;
-    const bool valid = i < A.n;
+    bool valid = i < A.n;
     // ---------------------------------------------------------------- features -> X
     {
       uint32_t w[Kp / 4];
       if (valid) {
-        const float2 uv = reinterpret_cast<const float2*>(A.uv)[i];
-        features<SH>(A, uv.x, uv.y, A.lod[i], w);
+        float u, v;
+        int lod;
+        if (A.screen_w > 0) {
+          valid = screen_sample(A, i, u, v, lod);
+        } else {
+          const float2 uv = reinterpret_cast<const float2*>(A.uv)[i];
+          u = uv.x;
+          v = uv.y;
+          lod = A.lod[i];
+        }
+        features<SH>(A, u, v, lod, w);
       } else {
 #pragma unroll
         for (int j = 0; j < Kp / 4; j++) w[j] = 0u;
@@ -418,13 +504,17 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::ld16(lwin, acc);
       ptx::ld_wait();
       if (valid) {
-        float* o = A.out + i * C;
 #pragma unroll
-        for (int c = 0; c < kOutRows; c++)
-          if (c < C) {
-            const float y = __fmul_rn((float)__float_as_int(acc[c]), so[c]);
-            o[c] = fminf(1.0f, fmaxf(0.0f, y));  // saturate
-          }
+        for (int c = 0; c < kOutRows; c++)  // saturate
+          acc[c] = fminf(1.0f, fmaxf(0.0f, __fmul_rn((float)__float_as_int(acc[c]), so[c])));
+        if (A.material) {
+          store_material(A.out + i * 18, acc, C, A);
+        } else {
+          float* o = A.out + i * C;
+#pragma unroll
+          for (int c = 0; c < kOutRows; c++)
+            if (c < C) o[c] = acc[c];
+        }
       }
     }
     // the next tile's features overwrite X only after every thread has read its outputs

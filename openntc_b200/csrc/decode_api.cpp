@@ -74,6 +74,60 @@ int upload_pyramid(uint32_t* const* levels, const size_t* sizes, const size_t* o
   return ONTC_SUCCESS;
 }
 
+ontc::DecodeArgs base_args(const ontc_decoder* d)
+{
+  ontc::DecodeArgs a;
+  a.g0 = d->g0;
+  a.g1 = d->g1;
+  a.g0_words = d->g0_words;
+  a.g1_words = d->g1_words;
+  a.blob = d->blob;
+  a.k = d->k;
+  a.err = d->err;
+  return a;
+}
+
+// DecodeMaterial (ntc_decode.hlsli:544-603) as a table: the ontc_material_params float each
+// channel writes (-1: none) and the `present` bits.  Field offsets: albedo 0-2, alpha 3,
+// displacement 4, emissive 5, gloss 6, metallic 7, normal 8-10, ao 11, roughness 12,
+// specular 13-15, transmission 16.
+void material_table(const ontc_constants& k, ontc::DecodeArgs& a)
+{
+  static_assert(sizeof(ontc_material_params) == 18 * 4, "MaterialParams is 18 words");
+  a.material = true;
+  a.material_present = 0;
+  uint32_t prev = 0;  // Semantic::None
+  int comp = 0;
+  for (int i = 0; i < 16; i++) {
+    a.material_dst[i] = -1;
+    if (i >= k.channel_count) continue;
+    const uint32_t sem = k.channel_semantics[i];
+    comp = sem == prev ? comp + 1 : 0;
+    prev = sem;
+    a.material_present |= 1u << (sem & 31u);  // HLSL shifts by the low 5 bits
+    const auto vec = [&](int base) { return comp < 3 ? base + comp : -1; };
+    switch (sem) {
+      case 1: a.material_dst[i] = (int8_t)vec(0); break;  // Albedo
+      case 2: a.material_dst[i] = 3; break;               // Alpha
+      case 3: a.material_dst[i] = 4; break;               // Displacement
+      case 4: a.material_dst[i] = 5; break;               // Emissive
+      case 5: a.material_dst[i] = 6; break;               // Gloss
+      case 6: a.material_dst[i] = 7; break;               // Metallic
+      case 7: a.material_dst[i] = (int8_t)vec(8); break;  // Normal
+      case 8: a.material_dst[i] = 11; break;              // AO
+      case 9: a.material_dst[i] = 12; break;              // Roughness
+      case 10: a.material_dst[i] = (int8_t)vec(13); break;  // Specular
+      case 11: a.material_dst[i] = 16; break;             // Transmission
+      default: break;
+    }
+  }
+}
+
+int launch(const ontc_decoder* d, const ontc::DecodeArgs& a)
+{
+  return ontc::launch_decode(d->profile, a, d->stream) == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
+}
+
 }  // namespace
 
 extern "C" {
@@ -137,19 +191,48 @@ void ontc_decoder_destroy(ontc_decoder* d)
 int ontc_decode(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out)
 {
   if (!d || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_out))) return ONTC_INVALID_STATE;
-  ontc::DecodeArgs a;
-  a.g0 = d->g0;
-  a.g1 = d->g1;
-  a.g0_words = d->g0_words;
-  a.g1_words = d->g1_words;
-  a.blob = d->blob;
-  a.k = d->k;
+  ontc::DecodeArgs a = base_args(d);
   a.uv = d_uv;
   a.lod = d_lod;
   a.n = n;
   a.out = d_out;
-  a.err = d->err;
-  return ontc::launch_decode(d->profile, a, d->stream) == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
+  return launch(d, a);
+}
+
+int ontc_decode_material(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n,
+                         ontc_material_params* d_params)
+{
+  if (!d || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_params))) return ONTC_INVALID_STATE;
+  if (reinterpret_cast<uintptr_t>(d_params) % 8 != 0) return ONTC_INVALID_STATE;
+  ontc::DecodeArgs a = base_args(d);
+  a.uv = d_uv;
+  a.lod = d_lod;
+  a.n = n;
+  a.out = reinterpret_cast<float*>(d_params);
+  material_table(d->k, a);
+  return launch(d, a);
+}
+
+int ontc_sample_screen(ontc_decoder* d, const float* d_uv, int32_t width, int32_t height, float noise_frame,
+                       int32_t flags, void* d_out)
+{
+  if (!d || width < 0 || height < 0 || (flags & ~(ONTC_SCREEN_DISCARD_OUTSIDE | ONTC_SCREEN_MATERIAL)))
+    return ONTC_INVALID_STATE;
+  if (width == 0 || height == 0) return ONTC_SUCCESS;
+  if (!d_uv || !d_out || reinterpret_cast<uintptr_t>(d_uv) % 8 != 0 ||
+      ((flags & ONTC_SCREEN_MATERIAL) && reinterpret_cast<uintptr_t>(d_out) % 8 != 0))
+    return ONTC_INVALID_STATE;
+  ontc::DecodeArgs a = base_args(d);
+  a.uv = d_uv;
+  a.lod = nullptr;
+  a.n = (int64_t)width * height;
+  a.out = static_cast<float*>(d_out);
+  a.screen_w = width;
+  a.screen_h = height;
+  a.noise_frame = noise_frame;
+  a.discard_outside = (flags & ONTC_SCREEN_DISCARD_OUTSIDE) != 0;
+  if (flags & ONTC_SCREEN_MATERIAL) material_table(d->k, a);
+  return launch(d, a);
 }
 
 int ontc_decoder_status(ontc_decoder* d)

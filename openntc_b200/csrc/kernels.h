@@ -24,8 +24,18 @@ struct DecodeArgs {
   const float* uv;      // [n][2]
   const int32_t* lod;   // [n]
   int64_t n;
-  float* out;           // [n][k.channel_count]
+  float* out;           // [n][k.channel_count], or ontc_material_params [n] when `material`
   int* err;             // set to 1 when a bounded wait gave up
+  // screen-space sampling (screen_w > 0): uv is a [screen_h][screen_w][2] image, lod unused,
+  // n = screen_w * screen_h, and each pixel's (uv, lod) comes from the stochastic filter
+  int32_t screen_w = 0, screen_h = 0;
+  float noise_frame = 0.0f;
+  bool discard_outside = false;
+  // DecodeMaterial output: material_dst[c] = float index in ontc_material_params written by
+  // channel c (-1: none); material_present = the `present` bits
+  bool material = false;
+  int8_t material_dst[16] = {};
+  uint32_t material_present = 0;
 };
 cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
 // one thread waits `polls` suspended polls on a barrier nothing arrives at; *d_out = 1 when it gave up

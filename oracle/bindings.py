@@ -69,6 +69,9 @@ class Oracle:
         L.orc_quantize_weights.argtypes = [P, C.c_int32, C.c_int32, C.c_float, P, P]
         L.orc_sample_material.argtypes = [C.c_int32, P, P, P, P, P, P, C.c_int64, P, C.c_int32]
         L.orc_decode_float.argtypes = [C.c_int32, P, P, P, P, C.c_int32, P, P, C.c_int64, P, C.c_int32]
+        L.orc_screen_filter.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_int32, P, P, P,
+                                        P, P]
+        L.orc_decode_material.argtypes = [P, C.c_int64, C.c_int32, P, P]
         L.orc_check_div3.argtypes = [C.c_int32]
         L.orc_check_div3.restype = C.c_int64
         self.L = L
@@ -165,6 +168,29 @@ class Oracle:
         out = np.zeros((len(lod), channels), np.float32)
         self.L.orc_sample_material(profile, _ptr(g0), _ptr(g1), _ptr(dec), _ptr(k), _ptr(uv), _ptr(lod), len(lod),
                                    _ptr(out), threads)
+        return out
+
+    def screen_filter(self, img, dim, mip_count, noise_frame, discard_outside=False):
+        """img float32 [h, w, 2] -> (uv [h*w, 2], lod [h*w], keep [h*w] bool, lod_ab [h*w], noise [h*w])."""
+        img = np.ascontiguousarray(img, np.float32)
+        h, w = img.shape[:2]
+        n = h * w
+        uv = np.zeros((n, 2), np.float32)
+        lod = np.zeros(n, np.int32)
+        keep = np.zeros(n, np.uint8)
+        lod_ab = np.zeros(n, np.float32)
+        noise = np.zeros(n, np.float32)
+        self.L.orc_screen_filter(_ptr(img), w, h, dim, mip_count, noise_frame, int(bool(discard_outside)), _ptr(uv),
+                                 _ptr(lod), _ptr(keep), _ptr(lod_ab), _ptr(noise))
+        return uv, lod, keep.astype(bool), lod_ab, noise
+
+    def decode_material(self, channels, semantics):
+        """channels float32 [n, C], semantics [C] -> float32 [n, 18] (the last word is `present`)."""
+        channels = np.ascontiguousarray(channels, np.float32)
+        sem = np.zeros(16, np.uint32)
+        sem[:len(semantics)] = semantics
+        out = np.zeros((len(channels), 18), np.float32)
+        self.L.orc_decode_material(_ptr(channels), len(channels), channels.shape[1], _ptr(sem), _ptr(out))
         return out
 
     def decode_float(self, profile, g0, g1, consts_bytes, W, channels, uv, lod, threads=8):

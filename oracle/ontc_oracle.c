@@ -575,6 +575,105 @@ void orc_sample_material(int32_t profile, const uint32_t* g0, const uint32_t* g1
   }
 }
 
+/* InterleavedGradientNoise (ntc_decode.hlsli:143-146); every operation rounded on its own. */
+static float ign_noise(float x, float y)
+{
+  const float t = 0.06711056f * x + 0.00583715f * y;
+  const float r = 52.9829189f * (t - floorf(t));
+  return r - floorf(r);
+}
+
+/* One uv component of the uv image [h][w][2] (pixel x, y). */
+static float uv_at(const float* img, int32_t w, int64_t x, int64_t y, int comp)
+{
+  return img[(y * w + x) * 2 + comp];
+}
+
+void orc_screen_filter(const float* img, int32_t w, int32_t h, int32_t dim, int32_t mip_count, float noise_frame,
+                       int32_t discard_outside, float* uv_out, int32_t* lod_out, uint8_t* keep, float* lod_ab,
+                       float* noise)
+{
+  const float fdim = (float)dim;
+  for (int64_t y = 0; y < h; y++)
+    for (int64_t x = 0; x < w; x++) {
+      const int64_t i = y * w + x;
+      const float u = uv_at(img, w, x, y, 0), v = uv_at(img, w, x, y, 1);
+      /* HLSL ddx/ddy (coarse): differences along the 2x2 quad's first row and first column */
+      const int64_t x0 = x - (x & 1), y0 = y - (y & 1);
+      float dx[2] = {0.0f, 0.0f}, dy[2] = {0.0f, 0.0f};
+      for (int c = 0; c < 2; c++) {
+        const float base = uv_at(img, w, x0, y0, c);
+        if (x0 + 1 < w)
+          dx[c] = uv_at(img, w, x0 + 1, y0, c) - base;
+        else if (x0 > 0)
+          dx[c] = base - uv_at(img, w, x0 - 1, y0, c);
+        if (y0 + 1 < h)
+          dy[c] = uv_at(img, w, x0, y0 + 1, c) - base;
+        else if (y0 > 0)
+          dy[c] = base - uv_at(img, w, x0, y0 - 1, c);
+      }
+      /* ComputeLod (ntc_decode.hlsli:152-168) */
+      const float dUdX[2] = {dx[0] * fdim, dx[1] * fdim}, dUdY[2] = {dy[0] * fdim, dy[1] * fdim};
+      const float gX = dUdX[0] * dUdX[0] + dUdX[1] * dUdX[1];
+      const float gY = dUdY[0] * dUdY[0] + dUdY[1] * dUdY[1];
+      const float* maj = gX > gY ? dUdX : dUdY;
+      const float foot[2] = {maj[0] / fdim, maj[1] / fdim};
+      float minor_axis = sqrtf(fminf(gX, gY));
+      const float major_axis = sqrtf(fmaxf(gX, gY));
+      minor_axis = fmaxf(minor_axis, major_axis / 8.0f);
+      const float lod = fminf(fmaxf(log2f(minor_axis), 0.0f), (float)(mip_count - 1));
+      /* noise position (flat_ntc.hlsl:82), StochasticFilterLod / StochasticFilterUv (:172-185) */
+      const float nf = 5.588238f * noise_frame;
+      const float px = ((float)x + 0.5f) + nf, py = ((float)y + 0.5f) + nf;
+      const float n1 = ign_noise(px, py);
+      lod_out[i] = (int32_t)lod + (n1 < lod - floorf(lod) ? 1 : 0);
+      const float j = ign_noise(px + 61.0f, py + 37.0f) - 0.5f;
+      uv_out[2 * i] = u + foot[0] * j;
+      uv_out[2 * i + 1] = v + foot[1] * j;
+      keep[i] = !(discard_outside && (u < 0.0f || v < 0.0f || u > 1.0f || v > 1.0f));
+      lod_ab[i] = lod;
+      noise[i] = n1;
+    }
+}
+
+void orc_decode_material(const float* channels, int64_t n, int32_t channel_count, const uint32_t* semantics,
+                         float* params)
+{
+  /* DefaultMaterialParams (ntc_decode.hlsli:524-540) then DecodeMaterial (:544-603) */
+  static const float def[17] = {0.5f, 0.5f, 0.5f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f, 0.5f,
+                                0.5f, 1.0f, 1.0f, 1.0f, 0.5f, 0.5f, 0.5f, 0.0f};
+  for (int64_t s = 0; s < n; s++) {
+    float* m = params + s * 18;
+    uint32_t present = 0;
+    memcpy(m, def, sizeof(def));
+    uint32_t prev = 0;
+    int comp = 0;
+    for (int i = 0; i < 16; i++) {
+      if (i >= channel_count) break;
+      const uint32_t sem = semantics[i];
+      comp = (sem == prev) ? comp + 1 : 0;
+      prev = sem;
+      present |= 1u << (sem & 31u);
+      const float v = channels[s * channel_count + i];
+      switch (sem) {
+        case 1: if (comp < 3) m[0 + comp] = v; break;  /* albedo_[comp] */
+        case 2: m[3] = v; break;
+        case 3: m[4] = v; break;
+        case 4: m[5] = v; break;
+        case 5: m[6] = v; break;
+        case 6: m[7] = v; break;
+        case 7: if (comp < 3) m[8 + comp] = v; break;  /* normal_[comp] */
+        case 8: m[11] = v; break;
+        case 9: m[12] = v; break;
+        case 10: if (comp < 3) m[13 + comp] = v; break; /* specular_[comp] */
+        case 11: m[16] = v; break;
+        default: break;
+      }
+    }
+    memcpy(m + 17, &present, 4);
+  }
+}
+
 void orc_decode_float(int32_t profile, const uint32_t* g0, const uint32_t* g1, const void* constants, const float* W,
                       int32_t C, const float* uv, const int32_t* lod, int64_t n, double* out, int32_t threads)
 {

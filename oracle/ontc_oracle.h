@@ -87,6 +87,21 @@ void orc_sample_material(int32_t profile, const uint32_t* g0, const uint32_t* g1
                          const void* constants, const float* uv, const int32_t* lod, int64_t n, float* out,
                          int32_t threads);
 
+/* The NTC pixel shaders' stochastic filter (flat_ntc.hlsl:74-84; ComputeLod,
+ * StochasticFilterLod, StochasticFilterUv, InterleavedGradientNoise at ntc_decode.hlsli:143-185)
+ * over a uv image img [h][w][2], with HLSL's coarse quad derivatives (backward difference where
+ * the image cuts a quad, 0 in a one-pixel dimension): per pixel the jittered uv, the chosen lod,
+ * whether it is kept (discard_outside: uv inside [0, 1]), the clamped float lod and the noise
+ * value the lod choice compared against. */
+void orc_screen_filter(const float* img, int32_t w, int32_t h, int32_t dim, int32_t mip_count, float noise_frame,
+                       int32_t discard_outside, float* uv_out, int32_t* lod_out, uint8_t* keep, float* lod_ab,
+                       float* noise);
+
+/* DecodeMaterial (ntc_decode.hlsli:524-603): saturated outputs [n][channel_count] and the
+ * per-channel semantics -> MaterialParams [n] as 17 floats + the `present` word. */
+void orc_decode_material(const float* channels, int64_t n, int32_t channel_count, const uint32_t* semantics,
+                         float* params);
+
 /* The float model decode (features from the packed latents dequantised, fp64 MLP with the
  * given fp32 weights), used as the FP64 decode reference. */
 void orc_decode_float(int32_t profile, const uint32_t* g0, const uint32_t* g1, const void* constants,
