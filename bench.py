@@ -8,11 +8,14 @@ moments.  A "step" is one optimisation step: draw -> gather -> MLP forward/backw
 latent scatter -> Adam over the whole current latent level.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision bf16|fp32]
-  python bench.py --workload decode [--steps K] [--warmup W]
+  python bench.py --workload decode [--steps K] [--warmup W] [--decode-input samples|screen]
 
 The decode workload times SampleMaterial over 3840 x 2160 x 8 = 66,355,200 samples (uv uniform
 in [0,1)^2, lod uniform in 0..12 clamped to 10) of a 4096^2 9-channel Bpp_2_25 material; a
-"step" is one decode of all samples.
+"step" is one decode of all samples.  With --decode-input screen the same number of samples
+are 8 stacked 3840 x 2160 frames of a receding textured plane (one 3840 x 17280 uv image), decoded
+by the screen-space sampler (quad derivatives -> lod -> stochastic lod and uv jitter ->
+SampleMaterial), a new noise frame every step.
 
 Prints one JSON line (rank 0).  `value` is device-timed with CUDA events on the library's
 stream (max over ranks); `e2e` is the same steps through the C ABI timed on the host,
@@ -300,8 +303,14 @@ def run_decode(args):
     torch.cuda.set_device(local)
     tmp = Path(tempfile.mkdtemp(prefix=f"ontc_decode_{rank}_"))
     cfg = dict(DECODE, dim=args.decode_dim or DECODE["dim"], samples=args.decode_samples or DECODE["samples"])
+    screen = args.decode_input == "screen"
     if cfg != DECODE:
         cfg["workload"] = f"decode_{cfg['dim']}sq_9ch_bpp2_25_n{cfg['samples']}"
+    if screen:
+        sw, sh = 3840, cfg["samples"] // 3840
+        assert sw * sh == cfg["samples"] and sh % 2 == 0
+        cfg["workload"] = f"screen_{cfg['dim']}sq_9ch_bpp2_25_{sw}x{sh}"
+        cfg["input"] = "uv image: 8 stacked 3840x2160 frames of a receding plane; noise frame = step"
     manifest = make_material(tmp / "set", cfg["dim"], DECODE["seed"] + rank, DECODE["channels"])
     ctx = ont.Context()
     assert ctx.init(DECODE["profile_id"]) == ont.Result.Success
@@ -314,34 +323,53 @@ def run_decode(args):
     g = torch.Generator(device="cuda").manual_seed(DECODE["seed"])
     uv = torch.rand((n, 2), device="cuda", generator=g)
     lod = torch.randint(0, 13, (n,), device="cuda", generator=g, dtype=torch.int32).clamp_(max=DECODE["lod_max"])
+    if screen:
+        rows = (torch.arange(sh, device="cuda", dtype=torch.float64) % 2160 + 0.5) / 2160
+        z = 1.0 / (0.02 + 0.98 * rows)[:, None]
+        cols = ((torch.arange(sw, device="cuda", dtype=torch.float64) + 0.5) / sw - 0.5)[None, :]
+        uv = torch.stack([0.5 + cols * z * 0.9, (z * 0.05).expand(sh, sw)], -1).float().contiguous()
     out = torch.empty((n, C), device="cuda")
     stream = torch.cuda.Stream()
     dec = ont.Decoder(cd, stream.cuda_stream)
+
+    def step(i, uv_ptr, out_ptr):
+        if screen:
+            return dec.sample_screen(uv_ptr, sw, sh, float(i), 0, out_ptr)
+        return dec.decode(uv_ptr, lod.data_ptr(), n, out_ptr)
+
     torch.cuda.synchronize()
     K, W = args.steps, args.warmup
-    for _ in range(W):
-        assert dec.decode(uv.data_ptr(), lod.data_ptr(), n, out.data_ptr()) == 0
+    for i in range(W):
+        assert step(i, uv.data_ptr(), out.data_ptr()) == 0
     assert dec.status() == 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
         ev0.record(stream)
-        for _ in range(K):
-            dec.decode(uv.data_ptr(), lod.data_ptr(), n, out.data_ptr())
+        for i in range(K):
+            step(W + i, uv.data_ptr(), out.data_ptr())
         ev1.record(stream)
         torch.cuda.synchronize()
     assert dec.status() == 0
     ms = ev0.elapsed_time(ev1) / K
     value = n / (ms / 1e3)
-    # e2e: host (pinned) samples in, host outputs back, through ontc_decode_host
-    h_uv, h_lod = uv.cpu().pin_memory(), lod.cpu().pin_memory()
+    # e2e: host (pinned) samples in, host outputs back
+    h_uv = uv.cpu().pin_memory()
+    h_lod = lod.cpu().pin_memory()
     h_out = torch.empty((n, C), pin_memory=True)
     lib = ont.load()
     t0 = time.perf_counter()
-    for _ in range(2):
-        assert lib.ontc_decode_host(dec.handle, h_uv.data_ptr(), h_lod.data_ptr(), n, h_out.data_ptr()) == 0
+    for i in range(2):
+        if screen:  # pinned copies on the decoder's stream around ontc_sample_screen
+            with torch.cuda.stream(stream):
+                d_uv = h_uv.to("cuda", non_blocking=True)
+                assert step(i, d_uv.data_ptr(), out.data_ptr()) == 0
+                h_out.copy_(out, non_blocking=True)
+            stream.synchronize()
+        else:  # through ontc_decode_host
+            assert lib.ontc_decode_host(dec.handle, h_uv.data_ptr(), h_lod.data_ptr(), n, h_out.data_ptr()) == 0
     e2e_s = (time.perf_counter() - t0) / 2
     pk = peaks()
-    bytes_per = 8 + 4 + 4 * C              # uv f32 x2 + lod i32 in, C f32 out
+    bytes_per = (8 if screen else 8 + 4) + 4 * C  # uv f32 x2 (+ lod i32) in, C f32 out
     ops_per = 2 * (64 * 92 + 64 * 64 + 9 * 64)  # int8 multiply-adds x 2 (F = 92 for Bpp_2_25)
     gbs = n * bytes_per / (ms / 1e3) / 1e9
     tops = n * ops_per / (ms / 1e3) / 1e12
@@ -364,27 +392,38 @@ def run_decode(args):
         k = bytes(ont.fill_constants(cd))
         m = 1 << 20
         threads = os.cpu_count() or 1
-        hu, hl = h_uv[:m].numpy(), h_lod[:m].numpy()
         t0 = time.perf_counter()
-        o.sample_material(cd.profile, pyramid(0), pyramid(1), blob, k, hu, hl, C, threads=threads)
+        if screen:  # the first 512 rows, filtered then decoded
+            img = h_uv[:512].numpy()
+            m = img.shape[0] * sw
+            fu, fl, _, _, _ = o.screen_filter(img, cd.dim, cd.mip_count, 0.0)
+            o.sample_material(cd.profile, pyramid(0), pyramid(1), blob, k, fu, fl, C, threads=threads)
+            what = f"oracle stochastic filter (1 thread) + SampleMaterial (OpenMP) on the first {m} pixels"
+        else:
+            hu, hl = h_uv[:m].numpy(), h_lod[:m].numpy()
+            o.sample_material(cd.profile, pyramid(0), pyramid(1), blob, k, hu, hl, C, threads=threads)
+            what = f"oracle SampleMaterial (C restatement of the DP4A path, OpenMP) on the first {m} samples"
         cs = time.perf_counter() - t0
-        cpu = {"value": round(m / cs, 1), "unit": "samples/s", "cores": threads, "kind": "port",
-               "sample": f"oracle SampleMaterial (C restatement of the DP4A path, OpenMP) on the first {m} samples"}
+        cpu = {"value": round(m / cs, 1), "unit": "samples/s", "cores": threads, "kind": "port", "sample": what}
     outl = {
         "metric": "decode samples/s", "value": round(value, 1), "unit": "samples/s", "n_gpus": 1, "steps": K,
         "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8 (s32 accumulate, fp32 requantisation)",
-        "data": "synthetic: seeded 4096^2 9-channel PBR set trained for a short schedule; seeded uv/lod",
+        "data": "synthetic: seeded 4096^2 9-channel PBR set trained for a short schedule; "
+                + ("a procedural uv image" if screen else "seeded uv/lod"),
         "config": dict(cfg, l2=f"inputs and outputs ({n * (12 + 4 * C) / 1e9:.2f} GB per step) vs 0.126 GB of L2"),
-        "roofline": {"bound": "hbm", "kernel": "decode_kernel (features, 3 int8 tcgen05 layers, requantisation)",
+        "roofline": {"bound": "hbm", "kernel": "decode_kernel (" + ("screen filter, " if screen else "")
+                     + "features, 3 int8 tcgen05 layers, requantisation)",
                      "achieved": round(gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"], "traffic": None,
                      "algorithmic_bytes_per_sample": bytes_per, "int8_tops": round(tops, 1),
                      "int8_tops_peak": round(2 * pk["bf16_tflops"], 1),
                      "note": "int8 peak taken as 2x the measured dense bf16 figure (spec ratio)"},
         "cpu_baseline": cpu,
-        "e2e": {"value": round(n / e2e_s, 1), "unit": "samples/s", "h2d_bytes_per_step": n * 12,
-                "d2h_bytes_per_step": n * 4 * C, "what": "ontc_decode_host from pinned host buffers"},
+        "e2e": {"value": round(n / e2e_s, 1), "unit": "samples/s", "h2d_bytes_per_step": n * (8 if screen else 12),
+                "d2h_bytes_per_step": n * 4 * C,
+                "what": ("ontc_sample_screen between pinned host copies on its stream" if screen
+                         else "ontc_decode_host from pinned host buffers")},
         "clocks": clk.summary(), "gpu_launches": K, "impl": "ours",
     }
     if rank == 0:
@@ -453,6 +492,8 @@ def main():
     ap.add_argument("--workload", choices=["train", "decode"], default="train")
     ap.add_argument("--decode-dim", type=int, default=0, help="decode material size (default 4096)")
     ap.add_argument("--decode-samples", type=int, default=0, help="samples per decode (default 66,355,200)")
+    ap.add_argument("--decode-input", choices=["samples", "screen"], default="samples",
+                    help="decode workload input: (uv, lod) lists or a uv image through the screen-space sampler")
     args = ap.parse_args()
     assert args.warmup >= 3
     if args.dim and args.dim != WORKLOAD["dim"]:
