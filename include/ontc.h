@@ -154,8 +154,20 @@ typedef struct ontc_train_options {
   int32_t precision;      /* ONTC_PRECISION_* */
   int32_t noise_mode;     /* ONTC_NOISE_* */
   int32_t latent_adam;    /* ONTC_LATENT_ADAM_* */
-  int32_t reserved[2];
+  int32_t calibration;    /* ONTC_CALIBRATION_* */
+  int32_t reserved;
 } ontc_train_options;
+
+/* How training completion chooses the int8 decoder's scales (same blob layout and .ntc format
+ * either way).
+ *   UPSTREAM (default): Calibrate's activation scales s_a = 1.1 max|activation| / 127 and
+ *                       per-row max weight scales (libopenntc.cpp:445-469, 898-970).
+ *   SEARCH:             the activation scales (multiples 0.8^k, k = 0..10, of upstream's) and
+ *                       per-row weight scales (max, or squared-error-optimal) that minimise the
+ *                       int8 decode's squared error against the training targets on a fixed
+ *                       sample of up to 2^21 texels over every mip; upstream's choice is one of
+ *                       the candidates.  The chosen s_a1 / s_a2 are the file's calibration. */
+enum { ONTC_CALIBRATION_UPSTREAM = 0, ONTC_CALIBRATION_SEARCH = 1 };
 
 /* How the latent Adam update of upstream (libopenntc.cpp:755-790: every latent of the step's
  * level, every step) is carried out.  Both give the same values.
@@ -209,6 +221,11 @@ int ontc_train_batch(ontc_context* const* ctxs, int32_t n, int32_t num_batches, 
 
 /* Context::Eval (libopenntc.cpp:972).  FP64 reduction. */
 void ontc_eval(ontc_context* ctx, ontc_eval_results* out);
+/* No upstream counterpart: the PSNR of the shipping int8 decode (ontc_decode at every texel
+ * centre of every mip, lod = the mip) against the training targets, with Eval's weighting and
+ * arithmetic (fp32 residual of target / 255, fp64 sums).  Only after training completes;
+ * failures set the sticky error (ontc_get_last_error) and return zeros, as ontc_eval does. */
+void ontc_eval_decoded(ontc_context* ctx, ontc_eval_results* out);
 /* Context::Calibrate (libopenntc.cpp:898) */
 void ontc_calibrate(ontc_context* ctx, float headroom, ontc_calibration* out);
 /* Context::GetCompressedData (libopenntc.cpp:1055) */

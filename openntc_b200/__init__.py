@@ -75,6 +75,11 @@ class LatentAdam(enum.IntEnum):
     DENSE = 1     # one pass over the whole level every step
 
 
+class CalibrationMode(enum.IntEnum):
+    UPSTREAM = 0  # Calibrate's 1.1 max / 127 activation scales, per-row max weight scales
+    SEARCH = 1    # scales chosen by the int8 decode's error on a texel sample
+
+
 class NoiseMode(enum.IntEnum):
     COUNTER = 0   # counter-based surrogate, generated at the touched latents only
     UPSTREAM = 1  # upstream's cuRAND stream and level-wide buffers (trajectory parity)
@@ -123,7 +128,8 @@ class Context:
 
     def begin_training(self, quality: int, grids_per_batch: int = 1, steps: int | None = None,
                        lock_step: int | None = None, precision: int = Precision.BF16,
-                       noise_mode: int = NoiseMode.COUNTER, latent_adam: int = LatentAdam.DEFERRED):
+                       noise_mode: int = NoiseMode.COUNTER, latent_adam: int = LatentAdam.DEFERRED,
+                       calibration: int = CalibrationMode.UPSTREAM):
         self._lib.ontc_begin_training(self._h, int(quality), int(grids_per_batch))
         o = TrainOptions()
         o.steps_override = steps or 0
@@ -132,6 +138,7 @@ class Context:
         o.precision = int(precision)
         o.noise_mode = int(noise_mode)
         o.latent_adam = int(latent_adam)
+        o.calibration = int(calibration)
         r = self._lib.ontc_set_train_options(self._h, C.byref(o))
         if r != 0:
             raise RuntimeError(f"ontc_set_train_options: {Result(r).name}")
@@ -149,6 +156,12 @@ class Context:
     def eval(self) -> EvalResults:
         r = EvalResults()
         self._lib.ontc_eval(self._h, C.byref(r))
+        return r
+
+    def eval_decoded(self) -> EvalResults:
+        """PSNR of the shipping int8 decode over every texel of every mip (after completion)."""
+        r = EvalResults()
+        self._lib.ontc_eval_decoded(self._h, C.byref(r))
         return r
 
     def calibrate(self, headroom: float = 1.1) -> Calibration:

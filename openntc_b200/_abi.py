@@ -84,7 +84,7 @@ class TextureData(C.Structure):
 class TrainOptions(C.Structure):
     _fields_ = [("steps_override", C.c_int32), ("has_lock_step", C.c_int32), ("lock_step", C.c_int32),
                 ("precision", C.c_int32), ("noise_mode", C.c_int32), ("latent_adam", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("calibration", C.c_int32), ("reserved", C.c_int32)]
 
 
 LATENT_ADAM_DEFERRED, LATENT_ADAM_DENSE = 0, 1
@@ -124,6 +124,7 @@ SIGNATURES = {
     "ontc_train": (None, [P, C.c_int32, C.POINTER(TrainProgress)]),
     "ontc_train_until_complete": (None, [P, C.POINTER(TrainProgress)]),
     "ontc_eval": (None, [P, C.POINTER(EvalResults)]),
+    "ontc_eval_decoded": (None, [P, C.POINTER(EvalResults)]),
     "ontc_calibrate": (None, [P, C.c_float, C.POINTER(Calibration)]),
     "ontc_get_compressed_data": (None, [P, C.POINTER(CompressedData)]),
     "ontc_get_texture_data": (None, [P, C.POINTER(TextureData)]),

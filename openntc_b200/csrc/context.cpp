@@ -21,6 +21,7 @@
 #include <cstring>
 #include <fstream>
 #include <iterator>
+#include <numeric>
 #include <random>
 #include <string>
 #include <vector>
@@ -98,6 +99,45 @@ void quantize_weights(const float* Wf, int rows, int cols, float prescale, uint3
   }
 }
 
+// The same int8 rows with each row's scale chosen to minimise the row's squared rounding
+// error sum_j (w_j - scale * q_j)^2 over scale = beta * max|w| / 127, beta = 1.00, 0.99, .. 0.60
+// (clipping the largest weights when that lowers the error); ties keep the larger scale.
+// No upstream counterpart (the calibration search below).
+void quantize_weights_mse(const float* Wf, int rows, int cols, float prescale, uint32_t* Wq, float* Ws)
+{
+  for (int i = 0; i < rows; i++) {
+    const float* w = Wf + (size_t)i * cols;
+    float max_abs = 0.0f;
+    for (int j = 0; j < cols; j++) max_abs = std::max(std::abs(w[j]), max_abs);
+    float best = (max_abs == 0.0f) ? 1.0f : max_abs / 127.0f;
+    if (max_abs != 0.0f) {
+      double best_err = -1.0;
+      for (int k = 0; k <= 40; k++) {
+        const float scale = (1.0f - 0.01f * (float)k) * max_abs / 127.0f;
+        double err = 0.0;
+        for (int j = 0; j < cols; j++) {
+          const int q = std::clamp((int)std::lroundf(w[j] / scale), -128, 127);
+          const double r = (double)w[j] - (double)scale * q;
+          err += r * r;
+        }
+        if (best_err < 0.0 || err < best_err) {
+          best_err = err;
+          best = scale;
+        }
+      }
+    }
+    Ws[i] = best * prescale;
+    for (int j = 0; j < cols; j += 4) {
+      uint32_t pack = 0;
+      for (int c = 0; c < 4; c++) {
+        const int q = std::clamp((int)std::lroundf(w[j + c] / best), -128, 127);
+        pack |= ((uint32_t)(q & 0xFF) << (c * 8));
+      }
+      Wq[i * (cols / 4) + (j / 4)] = pack;
+    }
+  }
+}
+
 // libopenntc.cpp:1103-1121
 bool valid_semantic_channels(int32_t sem, const std::string& ch)
 {
@@ -147,6 +187,7 @@ struct ontc_context {
   int32_t precision = ONTC_PRECISION_BF16;
   int32_t noise_mode = ONTC_NOISE_COUNTER;
   int32_t optimizer = ONTC_LATENT_ADAM_DEFERRED;
+  int32_t calibration = ONTC_CALIBRATION_UPSTREAM;
   int32_t upd_count[ONTC_MAX_LEVELS] = {};  // level steps with a latent update (before the lock)
   int32_t swept[ONTC_MAX_LEVELS] = {};      // every cell of the level has received this many
   int32_t lock_from[ONTC_MAX_LEVELS] = {}, lock_to[ONTC_MAX_LEVELS] = {};  // sweeps at the lock
@@ -553,6 +594,187 @@ ontc_calibration calibrate(ontc_context* c, float headroom, cudaError_t* err)
   return cal;
 }
 
+// The int8 decoder blob (libopenntc.cpp:841-876; layout DEC_*_OFFSET, ntc_decode.hlsli:95-103)
+// from the fp32 weights Wh with activation scales s_a1, s_a2: upstream's per-row max scales
+// (QuantizeWeights) or, with mse_weights, the per-row squared-error-optimal ones.
+void build_blob(const ontc_context* c, const std::vector<float>& Wh, float s_a1, float s_a2, bool mse_weights,
+                uint8_t* out)
+{
+  const int H = kHidden;
+  std::vector<float> W0pad((size_t)H * c->Fp, 0.0f);
+  for (int i = 0; i < H; i++) memcpy(&W0pad[(size_t)i * c->Fp], &Wh[(size_t)i * c->F], c->F * sizeof(float));
+  uint8_t* dec = out;
+  uint32_t* W0q = (uint32_t*)dec;
+  dec += H * c->Fp;
+  uint32_t* W1q = (uint32_t*)dec;
+  dec += H * H;
+  uint32_t* Woq = (uint32_t*)dec;
+  dec += kOutPad * H;
+  float* W0s = (float*)dec;
+  dec += H * sizeof(float);
+  float* W1s = (float*)dec;
+  dec += H * sizeof(float);
+  float* Wos = (float*)dec;
+  const auto q = mse_weights ? quantize_weights_mse : quantize_weights;
+  q(W0pad.data(), H, c->Fp, 1.0f / 128.0f, W0q, W0s);
+  q(&Wh[w1_off(c->F)], H, H, s_a1, W1q, W1s);
+  q(&Wh[wo_off(c->F)], c->C, H, s_a2, Woq, Wos);
+  memset(Woq + c->C * (H / 4), 0, (size_t)(kOutPad - c->C) * H);
+  for (int i = c->C; i < kOutPad; i++) Wos[i] = 0.0f;
+}
+
+// The context's mip chain and training targets as decode-evaluation texels.
+TexelMap texel_map(const ontc_context* c)
+{
+  TexelMap m;
+  m.mips = c->mips;
+  m.C = c->C;
+  for (int i = 0; i < c->mips; i++) {
+    m.dim[i] = c->mip_dim[i];
+    m.target[i] = c->package[i].p;
+    m.start[i + 1] = m.start[i] + (int64_t)c->mip_dim[i] * c->mip_dim[i];
+  }
+  return m;
+}
+
+// Device scratch of a decoded evaluation: `chunk` samples (uv, lod, outputs), fixed-grid
+// block partials and one fp64 sum per chunk.
+struct EvalScratch {
+  static constexpr int kBlocks = 512;
+  DBuf<float> uv, out;
+  DBuf<int32_t> lod;
+  DBuf<double> partial, sums;
+  cudaError_t alloc(int64_t chunk, int C, int chunks)
+  {
+    cudaError_t e = uv.alloc((size_t)chunk * 2);
+    if (!e) e = lod.alloc((size_t)chunk);
+    if (!e) e = out.alloc((size_t)chunk * C);
+    if (!e) e = partial.alloc(kBlocks);
+    if (!e) e = sums.alloc((size_t)chunks);
+    return e;
+  }
+};
+
+// sums[slot] = squared decode error of samples [j0, j0 + n) whose uv/lod are in the scratch.
+cudaError_t decode_sq_err(ontc_context* c, ontc_decoder* dec, const TexelMap& m, int64_t j0, int64_t n,
+                          EvalScratch& s, int slot)
+{
+  if (ontc_decode(dec, s.uv.p, s.lod.p, n, s.out.p) != ONTC_SUCCESS) return cudaErrorLaunchFailure;
+  cudaError_t e = launch_decoded_sq_err(m, j0, n, s.out.p, s.partial.p, EvalScratch::kBlocks, c->stream);
+  if (!e) e = launch_sum_doubles(s.partial.p, EvalScratch::kBlocks, s.sums.p + slot, c->stream);
+  c->launches += 3;
+  return e;
+}
+
+// A decoder of the context's completed material (latents as packed, current blob).
+cudaError_t context_decoder(ontc_context* c, ontc_decoder** dec)
+{
+  ontc_compressed_data cd;
+  ontc_get_compressed_data(c, &cd);
+  const int r = ontc_decoder_create(&cd, ONTC_DECODE_INT8, c->stream, dec);
+  return r == ONTC_SUCCESS ? cudaSuccess : (r == ONTC_ALLOCATION_FAILURE ? cudaErrorMemoryAllocation : cudaErrorUnknown);
+}
+
+// Squared decode error summed over every texel of every mip, in chunks of 4 M samples.
+cudaError_t decoded_sq_err_all(ontc_context* c, double* sum)
+{
+  ontc_decoder* dec = nullptr;
+  cudaError_t e = context_decoder(c, &dec);
+  if (e != cudaSuccess) return e;
+  const TexelMap m = texel_map(c);
+  const int64_t total = m.start[m.mips];
+  const int64_t chunk = std::min<int64_t>(total, 1 << 22);
+  const int chunks = (int)((total + chunk - 1) / chunk);
+  EvalScratch s;
+  e = s.alloc(chunk, c->C, chunks);
+  for (int k = 0; k < chunks && e == cudaSuccess; k++) {
+    const int64_t j0 = (int64_t)k * chunk, n = std::min(chunk, total - j0);
+    e = launch_texel_samples(m, j0, n, s.uv.p, s.lod.p, c->stream);
+    c->launches++;
+    if (!e) e = decode_sq_err(c, dec, m, j0, n, s, k);
+  }
+  std::vector<double> sums(chunks, 0.0);
+  if (!e) e = cudaMemcpyAsync(sums.data(), s.sums.p, chunks * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (!e && ontc_decoder_status(dec) != ONTC_SUCCESS) e = cudaErrorLaunchFailure;
+  ontc_decoder_destroy(dec);
+  *sum = 0.0;
+  for (double v : sums) *sum += v;
+  return e;
+}
+
+struct Calib {
+  float s_a1 = 0.0f, s_a2 = 0.0f;
+  bool mse_weights = false;
+};
+
+// ONTC_CALIBRATION_SEARCH (no upstream counterpart): the activation scales and the weight
+// rounding scales that minimise the int8 decode's squared error against the targets on a
+// fixed sample of up to 2^21 texels spread over every mip.  Coordinate descent over
+// s_a1 = a1 * s_a1(upstream), s_a2 = a2 * s_a2(upstream), a in {1, 0.8, 0.8^2, .., 0.8^10},
+// twice, then per-row weight scales (max or squared-error-optimal); upstream's choice
+// (a1 = a2 = 1, max weights) is the first candidate, so the result never scores worse on the
+// sample.  The blob layout and file format are unchanged.
+cudaError_t search_calibration(ontc_context* c, const std::vector<float>& Wh, Calib* best_out)
+{
+  const float base1 = c->caldata.s_a1, base2 = c->caldata.s_a2;
+  ontc_decoder* dec = nullptr;
+  cudaError_t e = context_decoder(c, &dec);
+  if (e != cudaSuccess) return e;
+  TexelMap m = texel_map(c);
+  const int64_t total = m.start[m.mips];
+  const int64_t n = std::min<int64_t>(total, 1 << 21);
+  if (n < total) {
+    int64_t stride = 2654435761ll;  // odd, > total: coprime once the gcd is 1
+    while (std::gcd(stride, total) != 1) stride += 2;
+    m.stride = stride;
+  }
+  EvalScratch s;
+  e = s.alloc(n, c->C, 1);
+  if (!e) e = launch_texel_samples(m, 0, n, s.uv.p, s.lod.p, c->stream);
+  c->launches++;
+  std::vector<uint8_t> blob(c->decoder_host.size());
+  auto score = [&](float a1, float a2, bool mw, double* err) -> cudaError_t {
+    build_blob(c, Wh, a1 * base1, a2 * base2, mw, blob.data());
+    if (ontc::decoder_set_weights(dec, blob.data(), blob.size(), a1 * base1, a2 * base2) != ONTC_SUCCESS)
+      return cudaErrorUnknown;
+    cudaError_t r = decode_sq_err(c, dec, m, 0, n, s, 0);
+    if (!r) r = cudaMemcpyAsync(err, s.sums.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (!r) r = cudaStreamSynchronize(c->stream);
+    return r;
+  };
+  float a[11];
+  a[0] = 1.0f;
+  for (int i = 1; i < 11; i++) a[i] = a[i - 1] * 0.8f;
+  float b1 = 1.0f, b2 = 1.0f;
+  bool bw = false;
+  double best = 0.0;
+  if (!e) e = score(b1, b2, bw, &best);
+  for (int pass = 0; pass < 2 && !e; pass++)
+    for (int axis = 0; axis < 2 && !e; axis++)
+      for (int i = 0; i < 11 && !e; i++) {
+        const float t1 = axis == 0 ? a[i] : b1, t2 = axis == 1 ? a[i] : b2;
+        if (t1 == b1 && t2 == b2) continue;
+        double err = 0.0;
+        e = score(t1, t2, bw, &err);
+        if (!e && err < best) {
+          best = err;
+          b1 = t1;
+          b2 = t2;
+        }
+      }
+  if (!e) {
+    double err = 0.0;
+    e = score(b1, b2, true, &err);
+    if (!e && err < best) bw = true;
+  }
+  if (!e && ontc_decoder_status(dec) != ONTC_SUCCESS) e = cudaErrorLaunchFailure;
+  ontc_decoder_destroy(dec);
+  best_out->s_a1 = b1 * base1;
+  best_out->s_a2 = b2 * base2;
+  best_out->mse_weights = bw;
+  return e;
+}
+
 // Training completion (libopenntc.cpp:799-876).
 cudaError_t complete_training(ontc_context* c)
 {
@@ -577,25 +799,15 @@ cudaError_t complete_training(ontc_context* c)
   std::vector<float> Wh(c->nW);
   e = cudaMemcpy(Wh.data(), c->W.p, c->nW * sizeof(float), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
-  const int H = kHidden;
-  std::vector<float> W0pad((size_t)H * c->Fp, 0.0f);
-  for (int i = 0; i < H; i++) memcpy(&W0pad[(size_t)i * c->Fp], &Wh[(size_t)i * c->F], c->F * sizeof(float));
-  uint8_t* dec = c->decoder_host.data();
-  uint32_t* W0q = (uint32_t*)dec;
-  dec += H * c->Fp;
-  uint32_t* W1q = (uint32_t*)dec;
-  dec += H * H;
-  uint32_t* Woq = (uint32_t*)dec;
-  dec += kOutPad * H;
-  float* W0s = (float*)dec;
-  dec += H * sizeof(float);
-  float* W1s = (float*)dec;
-  dec += H * sizeof(float);
-  float* Wos = (float*)dec;
-  quantize_weights(W0pad.data(), H, c->Fp, 1.0f / 128.0f, W0q, W0s);
-  quantize_weights(&Wh[w1_off(c->F)], H, H, c->caldata.s_a1, W1q, W1s);
-  quantize_weights(&Wh[wo_off(c->F)], c->C, H, c->caldata.s_a2, Woq, Wos);
-  for (int i = c->C; i < kOutPad; i++) Wos[i] = 0.0f;
+  build_blob(c, Wh, c->caldata.s_a1, c->caldata.s_a2, false, c->decoder_host.data());
+  if (c->calibration == ONTC_CALIBRATION_SEARCH && c->caldata.s_a1 > 0.0f && c->caldata.s_a2 > 0.0f) {
+    Calib best;
+    e = search_calibration(c, Wh, &best);
+    if (e != cudaSuccess) return e;
+    c->caldata.s_a1 = best.s_a1;
+    c->caldata.s_a2 = best.s_a2;
+    build_blob(c, Wh, best.s_a1, best.s_a2, best.mse_weights, c->decoder_host.data());
+  }
   return cudaSuccess;
 }
 
@@ -932,6 +1144,8 @@ int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
   if (o->has_lock_step) c->lock_i = std::max(0, o->lock_step);
   if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
   if (o->latent_adam != ONTC_LATENT_ADAM_DEFERRED && o->latent_adam != ONTC_LATENT_ADAM_DENSE) return ONTC_INVALID_STATE;
+  if (o->calibration != ONTC_CALIBRATION_UPSTREAM && o->calibration != ONTC_CALIBRATION_SEARCH) return ONTC_INVALID_STATE;
+  c->calibration = o->calibration;
   // the deferred kernels are compiled per profile channel pair; anything else runs dense
   c->optimizer = deferred_supported(c->C0, c->C1) ? o->latent_adam : ONTC_LATENT_ADAM_DENSE;
   c->noise_mode = o->noise_mode;
@@ -1237,6 +1451,24 @@ void ontc_eval(ontc_context* c, ontc_eval_results* out)
     num += sums[m];
     den += (double)c->mip_dim[m] * c->mip_dim[m] * c->C;
   }
+  out->mse = num / den;
+  out->psnr = -10.0 * std::log10(out->mse);
+}
+
+void ontc_eval_decoded(ontc_context* c, ontc_eval_results* out)
+{
+  *out = ontc_eval_results{};
+  if (!c->manifest_loaded || c->train_phase != ONTC_TRAIN_COMPLETE) {
+    c->last_error = ONTC_INVALID_STATE;
+    return;
+  }
+  double num = 0.0;
+  if (decoded_sq_err_all(c, &num) != cudaSuccess) {
+    c->last_error = ONTC_CUDA_FAILURE;
+    return;
+  }
+  double den = 0.0;
+  for (int m = 0; m < c->mips; m++) den += (double)c->mip_dim[m] * c->mip_dim[m] * c->C;
   out->mse = num / den;
   out->psnr = -10.0 * std::log10(out->mse);
 }

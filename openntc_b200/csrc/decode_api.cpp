@@ -130,6 +130,22 @@ int launch(const ontc_decoder* d, const ontc::DecodeArgs& a)
 
 }  // namespace
 
+namespace ontc {
+
+int decoder_set_weights(ontc_decoder* d, const uint8_t* blob, size_t size, float s_a1, float s_a2)
+{
+  ProfileShape ps;
+  if (!d || !blob || !profile_shape(d->profile, ps) || size != blob_bytes(ps)) return ONTC_INVALID_STATE;
+  if (cudaStreamSynchronize(d->stream) != cudaSuccess ||
+      cudaMemcpy(d->blob, blob, size, cudaMemcpyHostToDevice) != cudaSuccess)
+    return ONTC_CUDA_FAILURE;
+  d->k.rcp_s_a1 = 1.0f / s_a1;  // as FillNTCConstants forms them (openntc_runtime.cpp)
+  d->k.rcp_s_a2 = 1.0f / s_a2;
+  return ONTC_SUCCESS;
+}
+
+}  // namespace ontc
+
 extern "C" {
 
 int ontc_decoder_create(const ontc_compressed_data* data, int32_t mode, void* stream, ontc_decoder** out)

@@ -38,6 +38,25 @@ struct DecodeArgs {
   uint32_t material_present = 0;
 };
 cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
+// Replaces a decoder's int8 blob and activation scales (same layout and shapes); waits for its
+// stream first.  ONTC_* status.
+int decoder_set_weights(ontc_decoder* dec, const uint8_t* blob, size_t size, float s_a1, float s_a2);
+
+// The mip chain's texels as one sequence (mip 0 first, row-major); sample j is texel
+// (j * stride + offset) mod start[mips], stride coprime with the total and j * stride < 2^63.
+struct TexelMap {
+  int mips = 0, C = 0;
+  int dim[ONTC_MAX_MIPS] = {};
+  int64_t start[ONTC_MAX_MIPS + 1] = {};
+  const uint8_t* target[ONTC_MAX_MIPS] = {};  // [dim][dim][C] u8 training targets
+  int64_t stride = 1, offset = 0;
+};
+// uv (texel centre) and lod (its mip) of samples j0 .. j0 + n - 1
+cudaError_t launch_texel_samples(const TexelMap& m, int64_t j0, int64_t n, float* uv, int32_t* lod,
+                                 cudaStream_t stream);
+// partial[b] = sum over block b's samples of (target / 255 - out)^2, fp32 residuals, fp64 sums
+cudaError_t launch_decoded_sq_err(const TexelMap& m, int64_t j0, int64_t n, const float* out, double* partial,
+                                  int blocks, cudaStream_t stream);
 // one thread waits `polls` suspended polls on a barrier nothing arrives at; *d_out = 1 when it gave up
 cudaError_t launch_wait_check(uint32_t polls, int* d_out, cudaStream_t stream);
 

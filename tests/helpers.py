@@ -76,7 +76,7 @@ def make_step(lod, origins, noise=0, seed=0, step=0) -> _abi.DebugStep:
 
 def new_context(profile: int, manifest, min_dim: int = 16, quality: int = 0, grids: int = 1, steps=None,
                 lock_step=None, precision=ont.Precision.FP32, noise_mode=ont.NoiseMode.COUNTER,
-                latent_adam=ont.LatentAdam.DEFERRED) -> ont.Context:
+                latent_adam=ont.LatentAdam.DEFERRED, calibration=ont.CalibrationMode.UPSTREAM) -> ont.Context:
     ctx = ont.Context()
     r = ctx.init(profile)
     assert r == ont.Result.Success, r
@@ -84,7 +84,7 @@ def new_context(profile: int, manifest, min_dim: int = 16, quality: int = 0, gri
     r = ctx.load_manifest(manifest)
     assert r == ont.Result.Success, r
     ctx.begin_training(quality, grids, steps=steps, lock_step=lock_step, precision=precision, noise_mode=noise_mode,
-                       latent_adam=latent_adam)
+                       latent_adam=latent_adam, calibration=calibration)
     return ctx
 
 
