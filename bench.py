@@ -250,12 +250,18 @@ def run_ours(args):
     }
     for k in kernels.values():
         k["frac"] = round(k["achieved"] / k["peak"], 4) if k["peak"] else None
+    # deferred-optimiser work on the low-priority side stream, overlapped with the tile kernels
+    # (not part of the step's critical path, so not in the shares above)
+    side_cu, side_up = kt[_abi.KCLASS_SIDE_CATCHUP], kt[_abi.KCLASS_SIDE_UPDATE]
+    side = {"name": "next step's catch-up + this step's update outside the next footprint (side stream)",
+            "overlapped": True, "launches_per_step": (side_cu.launches + side_up.launches) / K,
+            "catchup_span_us": per_launch(side_cu), "update_span_us": per_launch(side_up)}
     dominant = max(("tile", "adam", "catchup"), key=lambda n: kernels[n]["share_of_step"])
     d = kernels[dominant]
     roofline = {"bound": d["bound"], "kernel": d["name"], "achieved": d["achieved"], "peak": d["peak"],
                 "unit": d["unit"], "frac": d["frac"], "peak_src": pk["src"], "traffic": d["traffic"],
                 "avg_launch_us": d["avg_launch_us"], "share_of_step": d["share_of_step"],
-                "kernels": kernels}
+                "kernels": kernels, "side_stream": side}
 
     out = None
     if rank == 0:

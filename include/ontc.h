@@ -10,8 +10,11 @@
  *
  * Conventions
  *  - Status returns are upstream's openntc::Result values (openntc_runtime.h:18-30).
- *  - One context = one GPU = one CUDA stream.  Not thread-safe; callers serialise, as
- *    upstream's GUI does (openntc-gui/thread.h:15-28).
+ *  - One context = one GPU = one CUDA stream (the caller's, or the library's own at the
+ *    highest priority).  Training also uses a private lowest-priority stream for deferred
+ *    optimiser work that overlaps the tile kernels; it is joined back into the context's
+ *    stream (by an event wait) before every training call returns.  Not thread-safe; callers
+ *    serialise, as upstream's GUI does (openntc-gui/thread.h:15-28).
  *  - All compute runs on hand-written sm_100a kernels inside libontc.so.  There is no
  *    CPU fallback: with no usable GPU, ontc_init returns ONTC_CUDA_FAILURE.
  */
@@ -174,7 +177,9 @@ enum { ONTC_CALIBRATION_UPSTREAM = 0, ONTC_CALIBRATION_SEARCH = 1 };
  *   DEFERRED (default): only the latents a step touches are updated in the step; the
  *                       zero-gradient steps the others miss are replayed (same arithmetic)
  *                       before they are next read, in level sweeps, at the lock and before
- *                       ontc_train returns.
+ *                       ontc_train returns.  The next step's replays outside this step's
+ *                       footprint, and this step's updates outside the next one's, run on the
+ *                       private stream beside the tile kernels.
  *   DENSE:              one pass over the whole level every step. */
 enum { ONTC_LATENT_ADAM_DEFERRED = 0, ONTC_LATENT_ADAM_DENSE = 1 };
 
@@ -349,11 +354,14 @@ enum {
   ONTC_KCLASS_UNITS_BF16 = 1, /* the same, tcgen05 bf16 */
   ONTC_KCLASS_ADAM = 2,       /* fused decoder + latent Adam / clamp / gradient-zero pass */
   ONTC_KCLASS_CATCHUP = 3,    /* deferred optimiser: footprint catch-up and level sweeps */
-  ONTC_KCLASS_COUNT = 4
+  ONTC_KCLASS_SIDE_CATCHUP = 4, /* the next step's catch-up, on the side stream beside a tile kernel */
+  ONTC_KCLASS_SIDE_UPDATE = 5,  /* a step's footprint update outside the next footprint, side stream */
+  ONTC_KCLASS_COUNT = 6
 };
 typedef struct ontc_kernel_time {
   int64_t launches;
-  double total_ms; /* sum of CUDA-event durations on the context's stream */
+  double total_ms; /* sum of CUDA-event durations on the stream the launches ran on (side-stream
+                      spans overlap the tile kernels they run beside) */
   double bytes;    /* algorithmic DRAM bytes of those launches */
   double flops;    /* algorithmic flops of those launches */
 } ontc_kernel_time;

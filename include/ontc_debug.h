@@ -81,6 +81,11 @@ int ontc_debug_shape(ontc_context* ctx, int32_t* out32);
  * in[k] = {x0, y0, x1, y1} -> disjoint rectangles with the same union in out (4 ints each).
  * Returns their count, or -1 when more than cap are needed. */
 int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap);
+/* The same cover of the cells of a[0..na) that lie (op 1) or do not lie (op 2) in some
+ * rectangle of b[0..nb): how consecutive steps' footprints are split between the main and the
+ * side stream. */
+int ontc_debug_cover_op(const int32_t* a, int32_t na, const int32_t* b, int32_t nb, int32_t op, int32_t* out,
+                        int32_t cap);
 
 /* The bounded wait of the tcgen05 kernels, exercised: one GPU thread waits `polls` (1..1000)
  * suspended polls of up to ~100 us on a barrier nothing arrives at.  Returns ONTC_CUDA_FAILURE

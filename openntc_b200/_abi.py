@@ -97,7 +97,8 @@ class KernelTime(C.Structure):
     _fields_ = [("launches", C.c_int64), ("total_ms", C.c_double), ("bytes", C.c_double), ("flops", C.c_double)]
 
 
-KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_CATCHUP, KCLASS_COUNT = 0, 1, 2, 3, 4
+KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_CATCHUP = 0, 1, 2, 3
+KCLASS_SIDE_CATCHUP, KCLASS_SIDE_UPDATE, KCLASS_COUNT = 4, 5, 6
 
 
 class DebugStep(C.Structure):
@@ -155,6 +156,7 @@ SIGNATURES = {
     "ontc_debug_package": (C.c_int, [P, C.c_int32, C.c_void_p]),
     "ontc_debug_shape": (C.c_int, [P, C.c_void_p]),
     "ontc_debug_disjoint_cover": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "ontc_debug_cover_op": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]),
     "ontc_lanczos_down_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "ontc_debug_wait_timeout": (C.c_int, [C.c_int32]),
     "ontc_train_batch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TrainProgress)]),

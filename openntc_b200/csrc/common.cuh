@@ -55,7 +55,10 @@ struct FootRec {
   int16_t r[2][kMaxFootRects][4];   // x0, y0, w, h in cells
 };
 
-constexpr int kHistRing = 64;  // level steps a latent cell may lag behind its level
+// Ring of per-level-step Adam scalars (lr, bias1, bias2) replayed by the deferred optimiser.
+// A cell lags its level by at most 64 level steps (the sweep interval); entries are written
+// from the step records up to a batch of steps ahead, so the ring holds twice that.
+constexpr int kHistRing = 128;
 
 // One latent pyramid (g0 or g1), fp32 master copy plus Adam state, [dim][dim][C] row-major
 // per level, exactly upstream's layout (ntc_kernel.cu:127-129).

@@ -164,6 +164,15 @@ uint32_t step_seed(uint32_t step)
 
 }  // namespace
 
+// The cell rectangles (half-open {x0, y0, x1, y1}) a step's tiles touch in each pyramid, before
+// they are merged into a disjoint cover (FootRec); kept per step so consecutive steps'
+// footprints can be intersected and subtracted.
+struct FootIn {
+  int n[2] = {0, 0};
+  int r[2][4 * kMaxGrids][4] = {};
+  bool whole[2] = {false, false};  // the cover fell back to the whole level
+};
+
 struct ontc_context {
   bool initialized = false;
   bool manifest_loaded = false;
@@ -207,6 +216,13 @@ struct ontc_context {
   DBuf<int32_t> applied[2][ONTC_MAX_LEVELS];
   DBuf<float4> hist;
   FootRec* h_foots = nullptr;  // pinned staging
+  std::vector<FootIn> foot_in;  // per step of the chunk
+  // The deferred optimiser's work that the next tile kernel does not read (the next step's
+  // catch-up outside this step's footprint, this step's update outside the next one's) runs
+  // on `side`, at the lowest priority, beside the tile kernels; events order it.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_pre = nullptr, ev_tile = nullptr, ev_cu = nullptr, ev_side = nullptr;
+  bool side_pending = false;
   DBuf<uint8_t> package[ONTC_MAX_MIPS];
   DBuf<uint32_t> packbuf;
   DBuf<int> tc_error;
@@ -251,17 +267,17 @@ struct ontc_context {
     cudaEventCreate(&e);
     return e;
   }
-  void prof_begin()
+  void prof_begin(cudaStream_t on = nullptr)
   {
     if (!profiling) return;
     prof_a = get_event();
-    cudaEventRecord(prof_a, stream);
+    cudaEventRecord(prof_a, on ? on : stream);
   }
-  void prof_end(int cls, double bytes, double flops)
+  void prof_end(int cls, double bytes, double flops, cudaStream_t on = nullptr)
   {
     if (!profiling || !prof_a) return;
     cudaEvent_t b = get_event();
-    cudaEventRecord(b, stream);
+    cudaEventRecord(b, on ? on : stream);
     prof.push_back({cls, prof_a, b, bytes, flops});
     prof_a = nullptr;
   }
@@ -325,9 +341,11 @@ struct ontc_context {
 
 namespace {
 
-// Sweep interval in level steps: as late as the ring allows (measured: intervals of 8-64 level
-// steps give the same step time at 2048^2).
-constexpr int kSweepEvery = kHistRing;
+// Sweep interval in level steps (measured: intervals of 8-64 level steps give the same step time
+// at 2048^2).  A cell lags its level by at most this many steps; the hist ring holds twice as
+// many so entries written up to a batch of steps ahead never overwrite one a replay reads.
+constexpr int kSweepEvery = 64;
+static_assert(kHistRing >= 2 * kSweepEvery, "hist entries are written ahead of their updates");
 
 bool ensure_host_steps(ontc_context* c, size_t n)
 {
@@ -367,44 +385,62 @@ void foot_ranges(int o, int T, int D, int gd, int out[2][2], int& n)
   }
 }
 
-// Disjoint cover of the union of half-open rectangles in[k] = {x0, y0, x1, y1}: elementary
-// cells between consecutive distinct edges, runs of covered cells merged along x within each
-// band, runs identical to the previous band's merged along y.  Returns the count, or -1 past cap.
-int disjoint_cover(const int (*in)[4], int n, int (*out)[4], int cap)
+// Disjoint cover of the cells selected from two sets of half-open rectangles {x0, y0, x1, y1}:
+// kCoverUnion the cells in some rectangle of a; kCoverInter those also in some rectangle of b;
+// kCoverMinus those in a and in no rectangle of b.  Elementary cells lie between consecutive
+// distinct edges of both sets; runs of selected cells are merged along x within each band, and
+// runs identical to the previous band's along y.  Returns the count, or -1 past cap.
+enum { kCoverUnion = 0, kCoverInter = 1, kCoverMinus = 2 };
+int cover_op(const int (*a)[4], int na, const int (*b)[4], int nb, int op, int (*out)[4], int cap)
 {
+  if (op == kCoverUnion) nb = 0;
   std::vector<int> xs, ys;
-  for (int k = 0; k < n; k++) {
-    xs.push_back(in[k][0]);
-    xs.push_back(in[k][2]);
-    ys.push_back(in[k][1]);
-    ys.push_back(in[k][3]);
+  for (int pass = 0; pass < 2; pass++) {
+    const int (*r)[4] = pass == 0 ? a : b;
+    for (int k = 0; k < (pass == 0 ? na : nb); k++) {
+      xs.push_back(r[k][0]);
+      xs.push_back(r[k][2]);
+      ys.push_back(r[k][1]);
+      ys.push_back(r[k][3]);
+    }
   }
   std::sort(xs.begin(), xs.end());
   xs.erase(std::unique(xs.begin(), xs.end()), xs.end());
   std::sort(ys.begin(), ys.end());
   ys.erase(std::unique(ys.begin(), ys.end()), ys.end());
+  const int nx = (int)xs.size() - 1, ny = (int)ys.size() - 1;
+  if (nx <= 0 || ny <= 0) return 0;
+  // bit 1: inside a rectangle of a; bit 2: inside one of b
+  std::vector<uint8_t> mark((size_t)nx * ny, 0);
+  auto paint = [&](const int* r, uint8_t bit) {
+    const int ix0 = (int)(std::lower_bound(xs.begin(), xs.end(), r[0]) - xs.begin());
+    const int ix1 = (int)(std::lower_bound(xs.begin(), xs.end(), r[2]) - xs.begin());
+    const int iy0 = (int)(std::lower_bound(ys.begin(), ys.end(), r[1]) - ys.begin());
+    const int iy1 = (int)(std::lower_bound(ys.begin(), ys.end(), r[3]) - ys.begin());
+    for (int iy = iy0; iy < iy1; iy++)
+      for (int ix = ix0; ix < ix1; ix++) mark[(size_t)iy * nx + ix] |= bit;
+  };
+  for (int k = 0; k < na; k++) paint(a[k], 1);
+  for (int k = 0; k < nb; k++) paint(b[k], 2);
+  const uint8_t want = op == kCoverInter ? 3 : 1;
   struct Open { int ix0, ix1, band, out; };
   std::vector<Open> open;
   int m = 0;
-  for (size_t iy = 0; iy + 1 < ys.size(); iy++) {
-    size_t ix = 0;
-    while (ix + 1 < xs.size()) {
-      auto covered = [&](size_t i) {
-        for (int k = 0; k < n; k++)
-          if (in[k][0] <= xs[i] && xs[i + 1] <= in[k][2] && in[k][1] <= ys[iy] && ys[iy + 1] <= in[k][3]) return true;
-        return false;
-      };
+  for (int iy = 0; iy < ny; iy++) {
+    auto covered = [&](int ix) { return mark[(size_t)iy * nx + ix] == want || (op == kCoverUnion && mark[(size_t)iy * nx + ix]); };
+    int ix = 0;
+    while (ix < nx) {
       if (!covered(ix)) {
         ix++;
         continue;
       }
-      size_t ix1 = ix + 1;
-      while (ix1 + 1 < xs.size() && covered(ix1)) ix1++;
+      int ix1 = ix + 1;
+      while (ix1 < nx && covered(ix1)) ix1++;
       bool extended = false;
       for (Open& o : open)
-        if (o.band == (int)iy - 1 && o.ix0 == (int)ix && o.ix1 == (int)ix1) {
+        if (o.band == iy - 1 && o.ix0 == ix && o.ix1 == ix1) {
           out[o.out][3] = ys[iy + 1];
-          o.band = (int)iy;
+          o.band = iy;
           extended = true;
           break;
         }
@@ -414,7 +450,7 @@ int disjoint_cover(const int (*in)[4], int n, int (*out)[4], int cap)
         out[m][1] = ys[iy];
         out[m][2] = xs[ix1];
         out[m][3] = ys[iy + 1];
-        open.push_back({(int)ix, (int)ix1, (int)iy, m});
+        open.push_back({ix, ix1, iy, m});
         m++;
       }
       ix = ix1;
@@ -423,14 +459,38 @@ int disjoint_cover(const int (*in)[4], int n, int (*out)[4], int cap)
   return m;
 }
 
+// Disjoint cover of the union of in[0..n).
+int disjoint_cover(const int (*in)[4], int n, int (*out)[4], int cap)
+{
+  return cover_op(in, n, nullptr, 0, kCoverUnion, out, cap);
+}
+
+// Pyramid g of F from a disjoint rectangle list.
+void fill_foot(FootRec& F, int g, const int (*out)[4], int m)
+{
+  int cells = 0;
+  for (int k = 0; k < m; k++) {
+    F.r[g][k][0] = (int16_t)out[k][0];
+    F.r[g][k][1] = (int16_t)out[k][1];
+    F.r[g][k][2] = (int16_t)(out[k][2] - out[k][0]);
+    F.r[g][k][3] = (int16_t)(out[k][3] - out[k][1]);
+    F.start[g][k] = cells;
+    cells += (out[k][2] - out[k][0]) * (out[k][3] - out[k][1]);
+  }
+  F.n[g] = m;
+  F.cells[g] = cells;
+}
+
 // The footprint of a step (FootRec, common.cuh): per pyramid the disjoint cover of every
 // tile's cell rectangles, or the whole level when the cover needs too many rectangles.
-void make_foot(const ontc_context* c, const StepRec& s, FootRec& F)
+void make_foot(const ontc_context* c, const StepRec& s, FootRec& F, FootIn& fi)
 {
   F = FootRec();
+  fi = FootIn();
   for (int g = 0; g < 2; g++) {
     const int gd = g == 0 ? c->g0_dim[s.level] : c->g1_dim[s.level];
-    int in[4 * kMaxGrids][4], out[kMaxFootRects][4], n = 0;
+    int (*in)[4] = fi.r[g];
+    int out[kMaxFootRects][4], n = 0;
     for (int t = 0; t < s.n_grids; t++) {
       int xr[2][2], yr[2][2], nx, ny;
       foot_ranges(s.ox[t], s.tile_dim, s.mip_dim, gd, xr, nx);
@@ -444,24 +504,48 @@ void make_foot(const ontc_context* c, const StepRec& s, FootRec& F)
           n++;
         }
     }
+    fi.n[g] = n;
     int m = disjoint_cover(in, n, out, kMaxFootRects);
     if (m < 0) {
       out[0][0] = out[0][1] = 0;
       out[0][2] = out[0][3] = gd;
       m = 1;
+      fi.whole[g] = true;
     }
-    int cells = 0;
-    for (int k = 0; k < m; k++) {
-      F.r[g][k][0] = (int16_t)out[k][0];
-      F.r[g][k][1] = (int16_t)out[k][1];
-      F.r[g][k][2] = (int16_t)(out[k][2] - out[k][0]);
-      F.r[g][k][3] = (int16_t)(out[k][3] - out[k][1]);
-      F.start[g][k] = cells;
-      cells += (out[k][2] - out[k][0]) * (out[k][3] - out[k][1]);
-    }
-    F.n[g] = m;
-    F.cells[g] = cells;
+    fill_foot(F, g, out, m);
   }
+}
+
+// For consecutive latent-updating steps a -> b: `cross` = cells of both footprints (updated
+// for a before b's tile kernel), `rest` = a's cells outside b (updated for a beside b's tile
+// kernel), `ahead` = b's cells outside a (caught up for b beside a's tile kernel).  Steps on
+// different levels share no cell.  False when a cover needs more than kMaxFootRects rectangles
+// or a footprint fell back to the whole level.
+bool split_feet(const StepRec& sa, const FootRec& fa, const FootIn& ia, const StepRec& sb, const FootRec& fb,
+                const FootIn& ib, FootRec& cross, FootRec& rest, FootRec& ahead)
+{
+  cross = FootRec();
+  if (sa.level != sb.level) {
+    rest = fa;
+    ahead = fb;
+    return true;
+  }
+  rest = FootRec();
+  ahead = FootRec();
+  for (int g = 0; g < 2; g++) {
+    if (ia.whole[g] || ib.whole[g]) return false;
+    int out[kMaxFootRects][4];
+    int m = cover_op(ia.r[g], ia.n[g], ib.r[g], ib.n[g], kCoverInter, out, kMaxFootRects);
+    if (m < 0) return false;
+    fill_foot(cross, g, out, m);
+    m = cover_op(ia.r[g], ia.n[g], ib.r[g], ib.n[g], kCoverMinus, out, kMaxFootRects);
+    if (m < 0) return false;
+    fill_foot(rest, g, out, m);
+    m = cover_op(ib.r[g], ib.n[g], ia.r[g], ia.n[g], kCoverMinus, out, kMaxFootRects);
+    if (m < 0) return false;
+    fill_foot(ahead, g, out, m);
+  }
+  return true;
 }
 
 // Brings every latent of every level from level step from[l] up to to[l] (deferred optimiser).
@@ -823,6 +907,12 @@ void ontc_destroy(ontc_context* c)
   unload(c);
   if (c->h_steps) cudaFreeHost(c->h_steps);
   if (c->h_foots) cudaFreeHost(c->h_foots);
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
+  }
+  for (cudaEvent_t ev : {c->ev_pre, c->ev_tile, c->ev_cu, c->ev_side})
+    if (ev) cudaEventDestroy(ev);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -855,7 +945,12 @@ int ontc_init(ontc_context* c, int32_t profile, void* stream)
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
   } else {
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return ONTC_CUDA_FAILURE;
+    // the library's own stream at the highest priority: the tile kernels and the work they wait
+    // for go before the side stream's (lowest priority) whenever both have CTAs pending
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, greatest) != cudaSuccess)
+      return ONTC_CUDA_FAILURE;
     c->own_stream = true;
   }
   if (c->W.alloc(c->nW) || c->Wm.alloc(c->nW) || c->Wv.alloc(c->nW) || c->dWpart.alloc((size_t)c->max_grid * c->nW) ||
@@ -1173,6 +1268,41 @@ namespace {
 
 // Draws and enqueues the next chunk of steps toward `target` (at most 1024, ending before the
 // lock step so that the latents can be snapped first); returns without waiting for the GPU.
+// Makes `side` (lowest priority) and its events on first use.
+cudaError_t ensure_side(ontc_context* c)
+{
+  if (c->side) return cudaSuccess;
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (!e) e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least);
+  for (cudaEvent_t* ev : {&c->ev_pre, &c->ev_tile, &c->ev_cu, &c->ev_side})
+    if (!e) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  return e;
+}
+
+// Orders everything enqueued on `side` so far before what is enqueued on the main stream next.
+cudaError_t drain_side(ontc_context* c)
+{
+  if (!c->side_pending) return cudaSuccess;
+  c->side_pending = false;
+  cudaError_t e = cudaEventRecord(c->ev_side, c->side);
+  if (!e) e = cudaStreamWaitEvent(c->stream, c->ev_side, 0);
+  return e;
+}
+
+// Draws and enqueues the next chunk of steps (at most 1024, ending at the lock step).
+//
+// Per latent-updating step k of the deferred optimiser, when step k + 1 updates latents too
+// and needs no level sweep first (footprints F(k), F(k+1)):
+//   main: [catch-up of F(k) outside F(k-1): done on side] -> tile(k) -> decoder Adam + update
+//         of F(k) n F(k+1) -> tile(k+1) ...
+//   side: catch-up of F(k+1) \ F(k), beside tile(k), after the step records are uploaded;
+//         then, after tile(k), the update of F(k) \ F(k+1), beside tile(k+1).
+// The side kernels touch no latent the concurrent tile kernel or main-stream update reads or
+// writes, and every cell's updates and replays keep their order (the side stream is in order;
+// a cell of F(k+1) \ F(k) was last updated on side or before tile(k)), so the values are those
+// of the serial schedule bit for bit.  Otherwise step k runs serially on the main stream after
+// the side stream drains.
 cudaError_t enqueue_chunk(ontc_context* c, int target)
 {
   std::bernoulli_distribution dist_batch_type(0.05);
@@ -1187,12 +1317,19 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
   int cnt = std::min(chunk_cap, target - first);
   // a chunk ends at the lock step so the latents can be snapped before it runs
   if (first < c->lock_i && first + cnt > c->lock_i) cnt = c->lock_i - first;
-  // Steps are drawn, uploaded and launched kPrepBatch at a time, so the GPU starts after the
-  // first few and the host prepares the rest while it runs (every step has its own staging slot).
+  if ((int)c->foot_in.size() < chunk_cap) c->foot_in.resize(chunk_cap);
+  const bool deferred_mode = c->optimizer == ONTC_LATENT_ADAM_DEFERRED;
+  if (deferred_mode && !e) e = ensure_side(c);
+
+  // Steps are drawn in order, one ahead of the batch being launched (a step's lookahead needs
+  // the next footprint), uploaded and launched kPrepBatch at a time, so the GPU starts after
+  // the first few and the host prepares the rest while it runs (every step has its own slot).
   constexpr int kPrepBatch = 8;
+  int drawn = 0, uploaded = 0;
+  int ahead_step = -1;  // the step whose catch-up was enqueued on side
   for (int k0 = 0; k0 < cnt && e == cudaSuccess; k0 += kPrepBatch) {
     const int k1 = std::min(cnt, k0 + kPrepBatch);
-    for (int k = k0; k < k1; k++) {
+    for (int k = drawn; k < std::min(cnt, k1 + 1); k++) {
       const int bi = first + k;
       const bool draw_uniform = dist_batch_type(c->gen);
       const float U = dist_u(c->gen);
@@ -1235,35 +1372,43 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       if (s.grid_update) {
         c->upd_count[s.level] += 1;
         if (c->optimizer == ONTC_LATENT_ADAM_DEFERRED) {
-          // a cell may lag its level by at most kHistRing steps (the ring of step scalars); the
-          // level is swept every kSweepEvery level steps
+          // a cell may lag its level by at most kSweepEvery steps: the level is swept every
+          // kSweepEvery level steps
           if (s.gstep - c->swept[s.level] >= kSweepEvery) {
             s.sweep_from = c->swept[s.level];
             c->swept[s.level] = s.gstep;
           }
           s.gfloor = c->swept[s.level];
-          make_foot(c, s, c->h_foots[k]);
+          make_foot(c, s, c->h_foots[k], c->foot_in[k]);
         }
       }
       s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
       s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
       s.step = bi;
     }
-    e = cudaMemcpyAsync(c->steps.p + k0, c->h_steps + k0, (k1 - k0) * sizeof(StepRec), cudaMemcpyHostToDevice,
-                        c->stream);
+    drawn = std::max(drawn, std::min(cnt, k1 + 1));
+    e = cudaMemcpyAsync(c->steps.p + uploaded, c->h_steps + uploaded, (drawn - uploaded) * sizeof(StepRec),
+                        cudaMemcpyHostToDevice, c->stream);
+    if (!e && deferred_mode) {
+      e = launch_hist_write(M, c->steps.p, uploaded, drawn, c->stream);
+      c->launches++;
+    }
+    uploaded = drawn;
     for (int k = k0; k < k1 && e == cudaSuccess; k++) {
       const int bi = first + k;
       const StepRec& s = c->h_steps[k];
-      if (c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
+      const bool ahead = ahead_step == k;
+      if (!ahead) e = drain_side(c);
+      if (!e && c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
         // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
         for (int g = 0; g < 2 && e == cudaSuccess; g++)
           e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
                                 g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
         c->launches += 2;
       }
-      if (bi == c->lock_i) {
+      if (!e && bi == c->lock_i) {
         // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
-        if (!e && c->optimizer == ONTC_LATENT_ADAM_DEFERRED) e = sweep_levels(c, c->lock_from, c->lock_to);
+        if (deferred_mode) e = sweep_levels(c, c->lock_from, c->lock_to);
         for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
           e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
           if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
@@ -1272,9 +1417,9 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
         for (int g = 0; g < 2 && e == cudaSuccess; g++)
           if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
       }
-      const bool deferred = c->optimizer == ONTC_LATENT_ADAM_DEFERRED && s.grid_update;
+      const bool deferred = deferred_mode && s.grid_update;
       const FootRec& fr = c->h_foots[k];
-      if (deferred) {
+      if (deferred && !ahead) {
         if (s.sweep_from >= 0) {
           c->prof_begin();
           if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
@@ -1283,17 +1428,39 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
           c->launches++;
         }
         c->prof_begin();
-        if (!e) e = launch_catchup(M, c->steps.p, k, fr, c->stream);
+        if (!e) e = launch_catchup(M, c->steps.p, k, fr, false, c->stream);
         // reads and writes p, m, v of the footprint latents that lag
         c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
         c->launches++;
+      }
+      if (ahead && !e) e = cudaStreamWaitEvent(c->stream, c->ev_cu, 0);
+      // the next step's catch-up outside this footprint, on side beside this tile kernel
+      FootRec cross, rest, next_cu;
+      bool look = false;
+      if (deferred && k + 1 < drawn) {
+        const StepRec& n = c->h_steps[k + 1];
+        look = n.grid_update && n.sweep_from < 0 &&
+               split_feet(s, fr, c->foot_in[k], n, c->h_foots[k + 1], c->foot_in[k + 1], cross, rest, next_cu);
+      }
+      if (look && !e) {
+        e = cudaEventRecord(c->ev_pre, c->stream);  // after the record uploads and this step's catch-up
+        if (!e) e = cudaStreamWaitEvent(c->side, c->ev_pre, 0);
+        c->prof_begin(c->side);
+        if (!e) e = launch_catchup(M, c->steps.p, k + 1, next_cu, true, c->side);
+        c->prof_end(ONTC_KCLASS_SIDE_CATCHUP,
+                    24.0 * ((double)next_cu.cells[0] * c->C0 + (double)next_cu.cells[1] * c->C1), 0.0, c->side);
+        c->launches++;
+        if (!e) e = cudaEventRecord(c->ev_cu, c->side);
+        ahead_step = k + 1;
+        c->side_pending = true;
       }
       const int units = (s.texels + kTile - 1) / kTile;
       TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
       int grid = std::min(units, c->sms);
       int cls = ONTC_KCLASS_UNITS_FP32;
       c->prof_begin();
-      if (c->precision == ONTC_PRECISION_BF16) {
+      if (e) {
+      } else if (c->precision == ONTC_PRECISION_BF16) {
         grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
         cls = ONTC_KCLASS_UNITS_BF16;
         e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
@@ -1309,28 +1476,42 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
       c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
       c->launches++;
-      c->prof_begin();
       if (deferred) {
+        const FootRec& now = look ? cross : fr;
+        if (look && !e) e = cudaEventRecord(c->ev_tile, c->stream);
+        c->prof_begin();
         if (!e)
-          e = launch_footprint_update(M, c->steps.p, k, fr, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
-                                      c->stream);
+          e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
+                                      false, c->stream);
         // footprint latents: p, m, v, g in and out (32 B each)
-        c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
+        c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)now.cells[0] * c->C0 + (double)now.cells[1] * c->C1), 0.0);
+        c->launches++;
+        if (look) {
+          if (!e) e = cudaStreamWaitEvent(c->side, c->ev_tile, 0);
+          c->prof_begin(c->side);
+          if (!e)
+            e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, nullptr, 0, nullptr, true, c->side);
+          c->prof_end(ONTC_KCLASS_SIDE_UPDATE, 32.0 * ((double)rest.cells[0] * c->C0 + (double)rest.cells[1] * c->C1),
+                      0.0, c->side);
+          c->launches++;
+        }
       } else {
+        c->prof_begin();
         if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
         // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
         c->prof_end(ONTC_KCLASS_ADAM,
                     s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
                     0.0);
+        c->launches++;
       }
-      c->launches++;
       c->last_seed = s.seed;
       c->last_noise = s.noise != 0;
       c->last_step = s;
       c->batch_i = bi + 1;
     }
   }
-  return e;
+  const cudaError_t d = drain_side(c);
+  return e ? e : d;
 }
 
 // Ends a run of ontc_train chunks: every latent current, the stream drained and checked, the
@@ -1779,6 +1960,14 @@ int ontc_debug_wait_timeout(int32_t polls)
   if (!e) e = cudaMemcpy(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost);
   if (e) return ONTC_CUDA_FAILURE;
   return h == 1 ? ONTC_CUDA_FAILURE : ONTC_INVALID_STATE;  // the wait must have given up
+}
+
+int ontc_debug_cover_op(const int32_t* a, int32_t na, const int32_t* b, int32_t nb, int32_t op, int32_t* out,
+                        int32_t cap)
+{
+  if (op != kCoverInter && op != kCoverMinus) return -1;
+  return cover_op(reinterpret_cast<const int (*)[4]>(a), na, reinterpret_cast<const int (*)[4]>(b), nb, op,
+                  reinterpret_cast<int (*)[4]>(out), cap);
 }
 
 int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_t cap)

@@ -81,12 +81,17 @@ cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_id
                              const double* loss_partial, int grid, double* loss_out, cudaStream_t stream);
 // deferred latent optimiser (see optim.cu): catch the step's footprint up to its level step,
 // apply the step's gradient to the footprint (plus the decoder Adam), sweep a whole level
-cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+// `side`: the side-stream instance (64-thread CTAs, which fill SMs as tile CTAs retire);
+// otherwise 256-thread CTAs
+cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F, bool side,
                            cudaStream_t stream);
-// decoder Adam + loss reduction + the step's gradient on its footprint, one launch
+// the step's gradient on the footprint F and, with `decoder` (main instance only), the decoder
+// Adam + loss reduction; one launch
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
-                                    const float* dW_partial, const double* loss_partial, int grid,
-                                    double* loss_out, cudaStream_t stream);
+                                    bool decoder, const float* dW_partial, const double* loss_partial, int grid,
+                                    double* loss_out, bool side, cudaStream_t stream);
+// the hist-ring entries of steps [k0, k1) that update latents, from their step records
+cudaError_t launch_hist_write(const Model& M, const StepRec* d_steps, int k0, int k1, cudaStream_t stream);
 // every latent of `level` from level step max(applied, from) to J
 cudaError_t launch_sweep(const Model& M, int level, int from, int J, cudaStream_t stream);
 // whether the deferred kernels are compiled for this (C0, C1) pair

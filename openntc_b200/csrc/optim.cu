@@ -208,9 +208,16 @@ __device__ __forceinline__ bool foot_item(const FootRec& F, int i, const Model& 
   return true;
 }
 
-template <int C0, int C1>
-__global__ void __launch_bounds__(256) catchup_kernel(Model M, const StepRec* __restrict__ steps, int idx,
-                                                      const __grid_constant__ FootRec F)
+// kSide: the instance launched on the side stream, in 64-thread CTAs that fill SMs as tile
+// CTAs retire and between launches.  (A tile CTA leaves 1,024 registers free in each of the
+// SM's four sub-partitions, so only <= 32-register warps could sit beside it; capped at 32 the
+// side kernels did, but slowed the tile kernel by more than they saved: 0.157 vs 0.155 ms per
+// 2048^2 step.)
+constexpr int kSideThreads = 64;
+
+template <int C0, int C1, bool kSide>
+__global__ void __launch_bounds__(kSide ? kSideThreads : 256)
+    catchup_kernel(Model M, const StepRec* __restrict__ steps, int idx, const __grid_constant__ FootRec F)
 {
   const StepRec& s = steps[idx];
   const int lvl = s.level, j = s.gstep, fl = s.gfloor;
@@ -249,21 +256,19 @@ __global__ void __launch_bounds__(256) sweep_kernel(Model M, int lvl, int fl, in
 
 // Decoder Adam (CTAs [0, n_dec)) and the step's gradient on its footprint, every latent of
 // which is at level step gstep (the other CTAs).
-template <int C0, int C1>
-__global__ void __launch_bounds__(256) footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx,
-                                                               const __grid_constant__ FootRec F,
-                                                               const float* __restrict__ dW_partial,
-                                                               const double* __restrict__ loss_partial, int grid,
-                                                               double* __restrict__ loss_out, int n_dec)
+template <int C0, int C1, bool kSide>
+__global__ void __launch_bounds__(kSide ? kSideThreads : 256)
+    footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx, const __grid_constant__ FootRec F,
+                            const float* __restrict__ dW_partial, const double* __restrict__ loss_partial, int grid,
+                            double* __restrict__ loss_out, int n_dec)
 {
   const StepRec& s = steps[idx];
-  if ((int)blockIdx.x < n_dec) {
+  if (!kSide && (int)blockIdx.x < n_dec) {
     decoder_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
     return;
   }
   const int lvl = s.level, j = s.gstep;
   const int i = (blockIdx.x - n_dec) * blockDim.x + threadIdx.x;
-  if (i == 0) M.hist[lvl][j & (kHistRing - 1)] = make_float4(s.lr_grid, s.gb1, s.gb2, 0.0f);
   int g, cell, q;
   if (!foot_item<C0, C1>(F, i, M, lvl, g, cell, q)) return;
   if (g == 0)
@@ -271,6 +276,16 @@ __global__ void __launch_bounds__(256) footprint_update_kernel(Model M, const St
   else
     update_grp<Groups<C1>::W>(M.g1, lvl, (int64_t)cell * C1 + q * Groups<C1>::W, s.lr_grid, s.gb1, s.gb2);
   if (q == 0) M.applied[g][lvl][cell] = j + 1;  // no thread of this kernel reads the counters
+}
+
+// The (lr, bias1, bias2) of every latent-updating step of [k0, k1) into its level's ring, at
+// its level step (what the deferred replays read).
+__global__ void hist_write_kernel(Model M, const StepRec* __restrict__ steps, int k0, int k1)
+{
+  const int k = k0 + (int)threadIdx.x;
+  if (k >= k1) return;
+  const StepRec& s = steps[k];
+  if (s.grid_update) M.hist[s.level][s.gstep & (kHistRing - 1)] = make_float4(s.lr_grid, s.gb1, s.gb2, 0.0f);
 }
 
 __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* __restrict__ steps, int step_idx,
@@ -358,14 +373,18 @@ static int dec_blocks(const Model& M) { return (M.nW + 31) / 32; }
 // Profile channel pairs (C0, C1) with compiled deferred-optimiser kernels.
 #define ONTC_FOR_CHANNEL_PAIRS(X) X(8, 12) X(12, 20) X(12, 10) X(16, 12)
 
-cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
+cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F, bool side,
                            cudaStream_t stream)
 {
 #define X(a, b)                                                                                          \
   if (M.g0.channels == a && M.g1.channels == b) {                                                        \
     const int total = F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q;                             \
     if (total <= 0) return cudaSuccess;                                                                  \
-    catchup_kernel<a, b><<<(total + 255) / 256, 256, 0, stream>>>(M, d_steps, step_idx, F);             \
+    if (side)                                                                                            \
+      catchup_kernel<a, b, true><<<(total + kSideThreads - 1) / kSideThreads, kSideThreads, 0, stream>>>(  \
+          M, d_steps, step_idx, F);                                                                      \
+    else                                                                                                 \
+      catchup_kernel<a, b, false><<<(total + 255) / 256, 256, 0, stream>>>(M, d_steps, step_idx, F);      \
     return cudaGetLastError();                                                                           \
   }
   ONTC_FOR_CHANNEL_PAIRS(X)
@@ -374,21 +393,38 @@ cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx,
 }
 
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
-                                    const float* dW_partial, const double* loss_partial, int grid,
-                                    double* loss_out, cudaStream_t stream)
+                                    bool decoder, const float* dW_partial, const double* loss_partial, int grid,
+                                    double* loss_out, bool side, cudaStream_t stream)
 {
-  const int n_dec = dec_blocks(M);
+  // the decoder CTAs are 256 threads (decoder_block): a launch with them is the main instance
+  if (decoder && side) return cudaErrorInvalidValue;
+  const int n_dec = decoder ? dec_blocks(M) : 0;
 #define X(a, b)                                                                                          \
   if (M.g0.channels == a && M.g1.channels == b) {                                                        \
-    const int total = std::max(1, F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q);                \
-    const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                     \
-    footprint_update_kernel<a, b><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, loss_partial, \
-                                                              grid, loss_out, n_dec);                    \
+    const int total = F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q;                             \
+    if (side) {                                                                                          \
+      if (total <= 0) return cudaSuccess;                                                                \
+      footprint_update_kernel<a, b, true><<<(total + kSideThreads - 1) / kSideThreads, kSideThreads, 0,    \
+                                            stream>>>(M, d_steps, step_idx, F, nullptr, nullptr, 0, nullptr, 0); \
+    } else {                                                                                             \
+      const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                   \
+      if (blocks == 0) return cudaSuccess;                                                               \
+      footprint_update_kernel<a, b, false><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, \
+                                                                       loss_partial, grid, loss_out, n_dec); \
+    }                                                                                                    \
     return cudaGetLastError();                                                                           \
   }
   ONTC_FOR_CHANNEL_PAIRS(X)
 #undef X
   return cudaErrorNotSupported;
+}
+
+cudaError_t launch_hist_write(const Model& M, const StepRec* d_steps, int k0, int k1, cudaStream_t stream)
+{
+  if (k1 <= k0) return cudaSuccess;
+  if (k1 - k0 > 1024) return cudaErrorInvalidValue;
+  hist_write_kernel<<<1, k1 - k0, 0, stream>>>(M, d_steps, k0, k1);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_sweep(const Model& M, int level, int from, int J, cudaStream_t stream)

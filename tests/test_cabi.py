@@ -119,3 +119,35 @@ def test_disjoint_cover_keeps_the_union(lib):
     one = np.array([[0, 0, 8, 8], [4, 4, 12, 12], [20, 0, 24, 4]], np.int32)
     out = np.zeros((4, 4), np.int32)
     assert lib.ontc_debug_disjoint_cover(one.ctypes.data, 3, out.ctypes.data, 2) == -1
+
+
+def test_footprint_intersection_and_difference_covers(lib):
+    """Consecutive steps' footprints split into shared cells and cells of one step only: each
+    cover is disjoint and selects exactly the cells of A in (op 1) or outside (op 2) B."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+    dim = 64
+
+    def rects(n):
+        x0 = rng.integers(0, dim, n); y0 = rng.integers(0, dim, n)
+        x1 = np.minimum(dim, x0 + rng.integers(1, 40, n)); y1 = np.minimum(dim, y0 + rng.integers(1, 40, n))
+        return np.stack([x0, y0, x1, y1], 1).astype(np.int32).copy()
+
+    def grid(rs):
+        g = np.zeros((dim, dim), bool)
+        for a, b, c, d in rs:
+            g[b:d, a:c] = True
+        return g
+
+    for case in range(300):
+        A, B = rects(int(rng.integers(0, 9))), rects(int(rng.integers(0, 9)))
+        for op, want in ((1, grid(A) & grid(B)), (2, grid(A) & ~grid(B))):
+            out = np.zeros((512, 4), np.int32)
+            m = lib.ontc_debug_cover_op(A.ctypes.data, len(A), B.ctypes.data, len(B), op, out.ctypes.data, 512)
+            assert m >= 0
+            got = np.zeros((dim, dim), np.int32)
+            for a, b, c, d in out[:m]:
+                assert a < c and b < d
+                got[b:d, a:c] += 1
+            assert np.array_equal(got, want.astype(np.int32)), (case, op)
+    assert lib.ontc_debug_cover_op(A.ctypes.data, len(A), B.ctypes.data, len(B), 0, out.ctypes.data, 512) == -1
