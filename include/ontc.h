@@ -283,7 +283,10 @@ void ontc_decoder_destroy(ontc_decoder* dec);
  * range as upstream does), into d_out [n][channel_count] f32.  Enqueued on the decoder's
  * stream; returns once enqueued. */
 int ontc_decode(ontc_decoder* dec, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out);
-/* The same from HOST buffers: copies in, decodes, copies out, and returns when done. */
+/* The same from HOST buffers: copies in, decodes, copies out, and returns when done.  Works in
+ * chunks of 2^20 samples over three internal streams, so one chunk's copy in, another's decode
+ * and a third's copy out overlap (with pinned host buffers; pageable ones work, without the
+ * overlap); the decoder keeps 3 x 2^20 samples of device staging from the first call on. */
 int ontc_decode_host(ontc_decoder* dec, const float* uv, const int32_t* lod, int64_t n, float* out);
 /* Waits for the decoder's stream; ONTC_CUDA_FAILURE if a decode failed or timed out. */
 int ontc_decoder_status(ontc_decoder* dec);

@@ -1,6 +1,7 @@
 // C ABI of the batch decoder (include/ontc.h, "Decode"): one compressed material held on the
 // device, decoded with upstream's SampleMaterial arithmetic (ntc_decode.hlsli:605-623) by
 // launch_decode (decode.cu).  Upstream has no batch decode API: its decode is HLSL only.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -16,11 +17,16 @@ struct ontc_decoder {
   uint32_t g0_words = 0, g1_words = 0;
   uint8_t* blob = nullptr;
   int* err = nullptr;
-  // staging for ontc_decode_host, grown on demand
-  float* uv = nullptr;
-  int32_t* lod = nullptr;
-  float* out = nullptr;
-  int64_t cap = 0;
+  // ontc_decode_host's pipeline: kPipe streams, each with its own chunk of staging, so one
+  // chunk's copy in, another's decode and a third's copy out run at the same time
+  static constexpr int kPipe = 3;
+  static constexpr int64_t kChunk = 1 << 20;  // samples per chunk
+  cudaStream_t pipe[kPipe] = {};
+  cudaEvent_t ev_start = nullptr;
+  float* uv[kPipe] = {};
+  int32_t* lod[kPipe] = {};
+  float* out[kPipe] = {};
+  bool staged = false;
 };
 
 namespace {
@@ -52,9 +58,30 @@ void release(ontc_decoder* d)
   cudaFree(d->g1);
   cudaFree(d->blob);
   cudaFree(d->err);
-  cudaFree(d->uv);
-  cudaFree(d->lod);
-  cudaFree(d->out);
+  for (int i = 0; i < ontc_decoder::kPipe; i++) {
+    cudaFree(d->uv[i]);
+    cudaFree(d->lod[i]);
+    cudaFree(d->out[i]);
+    if (d->pipe[i]) cudaStreamDestroy(d->pipe[i]);
+  }
+  if (d->ev_start) cudaEventDestroy(d->ev_start);
+}
+
+// The pipeline's streams and chunk buffers (kChunk samples of uv, lod and C outputs each).
+int ensure_pipeline(ontc_decoder* d)
+{
+  if (d->staged) return ONTC_SUCCESS;
+  const size_t n = ontc_decoder::kChunk, C = (size_t)d->k.channel_count;
+  if (cudaEventCreateWithFlags(&d->ev_start, cudaEventDisableTiming) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  for (int i = 0; i < ontc_decoder::kPipe; i++) {
+    if (cudaStreamCreateWithFlags(&d->pipe[i], cudaStreamNonBlocking) != cudaSuccess) return ONTC_CUDA_FAILURE;
+    if (cudaMalloc(&d->uv[i], n * 2 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d->lod[i], n * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&d->out[i], n * C * sizeof(float)) != cudaSuccess)
+      return ONTC_ALLOCATION_FAILURE;
+  }
+  d->staged = true;
+  return ONTC_SUCCESS;
 }
 
 // One pyramid, its levels at their byte offsets, into a fresh device buffer.
@@ -265,28 +292,34 @@ int ontc_decode_host(ontc_decoder* d, const float* uv, const int32_t* lod, int64
 {
   if (!d || n < 0 || (n > 0 && (!uv || !lod || !out))) return ONTC_INVALID_STATE;
   if (n == 0) return ONTC_SUCCESS;
-  const int C = d->k.channel_count;
-  if (n > d->cap) {
-    cudaFree(d->uv);
-    cudaFree(d->lod);
-    cudaFree(d->out);
-    d->uv = nullptr;
-    d->lod = nullptr;
-    d->out = nullptr;
-    d->cap = 0;
-    if (cudaMalloc(&d->uv, (size_t)n * 2 * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&d->lod, (size_t)n * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&d->out, (size_t)n * C * sizeof(float)) != cudaSuccess)
-      return ONTC_ALLOCATION_FAILURE;
-    d->cap = n;
-  }
-  cudaError_t e = cudaMemcpyAsync(d->uv, uv, (size_t)n * 2 * sizeof(float), cudaMemcpyHostToDevice, d->stream);
-  if (!e) e = cudaMemcpyAsync(d->lod, lod, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, d->stream);
-  if (e) return ONTC_CUDA_FAILURE;
-  int r = ontc_decode(d, d->uv, d->lod, n, d->out);
+  int r = ensure_pipeline(d);
   if (r != ONTC_SUCCESS) return r;
-  if (cudaMemcpyAsync(out, d->out, (size_t)n * C * sizeof(float), cudaMemcpyDeviceToHost, d->stream) != cudaSuccess)
-    return ONTC_CUDA_FAILURE;
+  const int C = d->k.channel_count;
+  // the chunks start after whatever the caller enqueued on the decoder's stream before
+  cudaError_t e = cudaEventRecord(d->ev_start, d->stream);
+  for (int i = 0; i < ontc_decoder::kPipe && !e; i++) e = cudaStreamWaitEvent(d->pipe[i], d->ev_start, 0);
+  // chunk j on stream j % kPipe: in, decode, out; a stream reuses its buffers only after its
+  // previous chunk's copy out (stream order).  Host buffers in pinned memory let the copies
+  // of different chunks overlap each other and the decodes.
+  for (int64_t j0 = 0, j = 0; j0 < n && !e; j0 += ontc_decoder::kChunk, j++) {
+    const int p = (int)(j % ontc_decoder::kPipe);
+    const int64_t m = std::min<int64_t>(ontc_decoder::kChunk, n - j0);
+    e = cudaMemcpyAsync(d->uv[p], uv + 2 * j0, (size_t)m * 2 * sizeof(float), cudaMemcpyHostToDevice, d->pipe[p]);
+    if (!e) e = cudaMemcpyAsync(d->lod[p], lod + j0, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, d->pipe[p]);
+    if (!e) {
+      ontc::DecodeArgs a = base_args(d);
+      a.uv = d->uv[p];
+      a.lod = d->lod[p];
+      a.n = m;
+      a.out = d->out[p];
+      e = ontc::launch_decode(d->profile, a, d->pipe[p]);
+    }
+    if (!e)
+      e = cudaMemcpyAsync(out + j0 * C, d->out[p], (size_t)m * C * sizeof(float), cudaMemcpyDeviceToHost, d->pipe[p]);
+  }
+  for (int i = 0; i < ontc_decoder::kPipe; i++)
+    if (cudaStreamSynchronize(d->pipe[i]) != cudaSuccess) e = cudaErrorUnknown;
+  if (e) return ONTC_CUDA_FAILURE;
   return ontc_decoder_status(d);
 }
 

@@ -131,3 +131,28 @@ def test_decoder_rejects_mismatched_data(trained):
     assert lib.ontc_decoder_create(C.byref(bad), _abi.DECODE_INT8, None, C.byref(h)) == ont.Result.InvalidFile
     assert lib.ontc_decoder_create(C.byref(cd), 7, None, C.byref(h)) == ont.Result.InvalidState
     assert not h.value
+
+
+def test_host_decode_pipeline_spans_chunks(trained, oracle):
+    """ontc_decode_host in chunks of 2^20 samples over three streams: 3.4 M pinned samples (four
+    chunks, the buffers of the first reused by the last) equal the device-buffer decode bit for
+    bit, and the oracle on every 997th sample and on the chunk edges."""
+    torch = pytest.importorskip("torch")
+    cd = trained[ont.Profile.Bpp_2_25].get_compressed_data()
+    n = 3 * (1 << 20) + 400_003
+    uv, lod = samples(n, cd.mip_count, 21)
+    dec = ont.Decoder(cd)
+    h_uv, h_lod = torch.from_numpy(uv).pin_memory(), torch.from_numpy(lod).pin_memory()
+    h_out = torch.empty((n, cd.channel_count), dtype=torch.float32).pin_memory()
+    lib = ont.load()
+    assert lib.ontc_decode_host(dec.handle, h_uv.data_ptr(), h_lod.data_ptr(), n, h_out.data_ptr()) == 0
+    got = h_out.numpy()
+    d_out = torch.empty((n, cd.channel_count), device="cuda")
+    d_uv, d_lod = h_uv.cuda(), h_lod.cuda()
+    torch.cuda.synchronize()
+    assert dec.decode(d_uv.data_ptr(), d_lod.data_ptr(), n, d_out.data_ptr()) == 0 and dec.status() == 0
+    assert np.array_equal(got.view(np.uint32), d_out.cpu().numpy().view(np.uint32))
+    edges = np.array([(1 << 20) * k + o for k in range(1, 4) for o in (-1, 0)])
+    idx = np.unique(np.concatenate([np.arange(0, n, 997), edges, [n - 1]]))
+    want = oracle_decode(oracle, cd, uv[idx], lod[idx])
+    assert np.array_equal(got[idx].view(np.uint32), want.view(np.uint32))
