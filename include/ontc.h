@@ -350,6 +350,9 @@ int ontc_sample_screen(ontc_decoder* dec, const float* d_uv, int32_t width, int3
 
 /* Number of kernel launches this context issued so far (all of them are libontc's own). */
 int64_t ontc_kernel_launch_count(ontc_context* ctx);
+/* Texels trained so far by this context: the sum over launched steps of grids x min(mip, 256)^2
+ * for the step's drawn lod (a step whose mip is smaller than 256^2 trains fewer texels). */
+int64_t ontc_texels_trained(ontc_context* ctx);
 
 /* Kernel classes timed by ontc_profile_kernels. */
 enum {

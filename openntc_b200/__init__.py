@@ -198,6 +198,10 @@ class Context:
     def kernel_launches(self) -> int:
         return self._lib.ontc_kernel_launch_count(self._h)
 
+    def texels_trained(self) -> int:
+        """Texels actually trained so far (a step at a mip below 256^2 trains fewer)."""
+        return self._lib.ontc_texels_trained(self._h)
+
 
 class FileData:
     """openntc::FileData (openntc_runtime.h:131-150): owns a loaded container."""

@@ -144,6 +144,7 @@ SIGNATURES = {
     "ontc_semantic_from_name": (C.c_int32, [C.c_char_p]),
     "ontc_channel_count_for_semantic": (C.c_int32, [C.c_int32]),
     "ontc_kernel_launch_count": (C.c_int64, [P]),
+    "ontc_texels_trained": (C.c_int64, [P]),
     "ontc_version": (C.c_char_p, []),
     "ontc_profile_kernels": (C.c_int, [P, C.c_int32]),
     "ontc_kernel_times": (C.c_int, [P, C.POINTER(KernelTime), C.c_int32]),

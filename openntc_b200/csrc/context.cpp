@@ -243,6 +243,7 @@ struct ontc_context {
   std::vector<uint8_t> mips_host[ONTC_MAX_SOURCES][ONTC_MAX_MIPS];
 
   int64_t launches = 0;
+  int64_t texels_trained = 0;
   StepRec last_step = {};
 
   // optional per-kernel timing (ontc_profile_kernels): CUDA events around each launch on
@@ -1507,6 +1508,7 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       c->last_seed = s.seed;
       c->last_noise = s.noise != 0;
       c->last_step = s;
+      c->texels_trained += s.texels;
       c->batch_i = bi + 1;
     }
   }
@@ -1751,6 +1753,8 @@ int ontc_get_step_losses(ontc_context* c, double* out, int32_t n)
 }
 
 int64_t ontc_kernel_launch_count(ontc_context* c) { return c->launches; }
+
+int64_t ontc_texels_trained(ontc_context* c) { return c->texels_trained; }
 
 int ontc_profile_kernels(ontc_context* c, int32_t enable)
 {
