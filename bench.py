@@ -313,6 +313,7 @@ def run_decode(args):
     import numpy as np
     import torch
     import openntc_b200 as ont
+    from openntc_b200 import _abi
     from openntc_b200.synth import make_material
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
@@ -345,7 +346,15 @@ def run_decode(args):
         uv = torch.stack([0.5 + cols * z * 0.9, (z * 0.05).expand(sh, sw)], -1).float().contiguous()
     out = torch.empty((n, C), device="cuda")
     stream = torch.cuda.Stream()
-    dec = ont.Decoder(cd, stream.cuda_stream)
+    modes = {"int8": _abi.DECODE_INT8, "fp32": _abi.DECODE_FP32, "bf16": _abi.DECODE_BF16, "fp8": _abi.DECODE_FP8}
+    mode = args.decode_mode
+    if mode == "int8":
+        dec = ont.Decoder(cd, stream.cuda_stream)
+    else:  # the trained float model in place of the int8 blob
+        assert not screen, "the screen-space sampler runs the int8 decoder"
+        dec = ont.Decoder.from_context(ctx, modes[mode], stream.cuda_stream)
+        cfg["workload"] = cfg["workload"].replace("decode_", f"decode_{mode}_")
+    cfg["decoder"] = mode
 
     def step(i, uv_ptr, out_ptr):
         if screen:
@@ -389,6 +398,7 @@ def run_decode(args):
     gbs = n * bytes_per / (ms / 1e3) / 1e9
     tops = n * ops_per / (ms / 1e3) / 1e12
     cpu = None
+    errors = None
     if not args.no_cpu_baseline:
         import ctypes
         from oracle.bindings import Oracle
@@ -420,21 +430,39 @@ def run_decode(args):
             what = f"oracle SampleMaterial (C restatement of the DP4A path, OpenMP) on the first {m} samples"
         cs = time.perf_counter() - t0
         cpu = {"value": round(m / cs, 1), "unit": "samples/s", "cores": threads, "kind": "port", "sample": what}
+        if not screen:  # this decoder's outputs against the FP64 float decode, per channel
+            ne = 20000
+            ctx_nw = ctx._lib.ontc_debug_tensor(ctx.handle, _abi.DBG_W, 0, None, 0, 0)
+            Wf = np.zeros(ctx_nw, np.float32)
+            ctx._lib.ontc_debug_tensor(ctx.handle, _abi.DBG_W, 0, Wf.ctypes.data_as(ctypes.c_void_p), ctx_nw, 0)
+            ref = o.decode_float(cd.profile, pyramid(0), pyramid(1), k, Wf, C, h_uv[:ne].numpy(), h_lod[:ne].numpy(),
+                                 threads=threads)
+            err = np.abs(out[:ne].cpu().numpy().astype(np.float64) - ref)
+            errors = {"vs": "FP64 float decode (fp32 weights, dequantised latents, saturated)", "samples": ne,
+                      "max": [round(float(v), 6) for v in err.max(0)], "mean": [round(float(v), 7) for v in err.mean(0)]}
     outl = {
         "metric": "decode samples/s", "value": round(value, 1), "unit": "samples/s", "n_gpus": 1, "steps": K,
         "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int8 (s32 accumulate, fp32 requantisation)",
+        "vs_baseline": None,
+        "dtype": {"int8": "int8 (s32 accumulate, fp32 requantisation)", "fp32": "fp32 (CUDA cores)",
+                  "bf16": "bf16 (fp32 accumulate)", "fp8": "e4m3, per-layer scales (fp32 accumulate)"}[mode],
         "data": "synthetic: seeded 4096^2 9-channel PBR set trained for a short schedule; "
                 + ("a procedural uv image" if screen else "seeded uv/lod"),
         "config": dict(cfg, l2=f"inputs and outputs ({n * (12 + 4 * C) / 1e9:.2f} GB per step) vs 0.126 GB of L2"),
-        "roofline": {"bound": "hbm", "kernel": "decode_kernel (" + ("screen filter, " if screen else "")
-                     + "features, 3 int8 tcgen05 layers, requantisation)",
+        "roofline": {"bound": "hbm",
+                     "kernel": {"int8": "decode_kernel (" + ("screen filter, " if screen else "")
+                                + "features, 3 int8 tcgen05 layers, requantisation)",
+                                "fp32": "decode_f32_kernel (features, 3 fp32 layers on the CUDA cores)",
+                                "bf16": "decode_tc_kernel<bf16> (features, 3 tcgen05 kind::f16 layers)",
+                                "fp8": "decode_tc_kernel<e4m3> (features, 3 tcgen05 kind::f8f6f4 layers)"}[mode],
                      "achieved": round(gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(gbs / pk["hbm_gbs"], 4), "peak_src": pk["src"], "traffic": None,
-                     "algorithmic_bytes_per_sample": bytes_per, "int8_tops": round(tops, 1),
-                     "int8_tops_peak": round(2 * pk["bf16_tflops"], 1),
-                     "note": "int8 peak taken as 2x the measured dense bf16 figure (spec ratio)"},
+                     "algorithmic_bytes_per_sample": bytes_per, "tensor_tops": round(tops, 1),
+                     "tensor_tops_peak": (None if mode == "fp32" else
+                                          round((1 if mode == "bf16" else 2) * pk["bf16_tflops"], 1)),
+                     "note": "int8 / e4m3 peak taken as 2x the measured dense bf16 figure (spec ratio)"},
         "cpu_baseline": cpu,
+        "error_per_channel": errors,
         "e2e": {"value": round(n / e2e_s, 1), "unit": "samples/s", "h2d_bytes_per_step": n * (8 if screen else 12),
                 "d2h_bytes_per_step": n * 4 * C,
                 "what": ("ontc_sample_screen between pinned host copies on its stream" if screen
@@ -585,6 +613,8 @@ def main():
     ap.add_argument("--workload", choices=["train", "decode", "batch"], default="train")
     ap.add_argument("--decode-dim", type=int, default=0, help="decode material size (default 4096)")
     ap.add_argument("--decode-samples", type=int, default=0, help="samples per decode (default 66,355,200)")
+    ap.add_argument("--decode-mode", choices=["int8", "fp32", "bf16", "fp8"], default="int8",
+                    help="decoder: the shipping int8 blob, or the trained float model in fp32 / bf16 / fp8")
     ap.add_argument("--decode-input", choices=["samples", "screen"], default="samples",
                     help="decode workload input: (uv, lod) lists or a uv image through the screen-space sampler")
     args = ap.parse_args()

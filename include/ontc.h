@@ -66,7 +66,13 @@ enum { ONTC_PRECISION_BF16 = 0, ONTC_PRECISION_FP32 = 1 };
 
 /* Decoder arithmetic for ontc_decode (upstream: HLSL only, ntc_decode.hlsli:605-623). */
 enum {
-  ONTC_DECODE_INT8 = 0 /* SampleMaterial semantics, integer-exact with the DP4A path */
+  ONTC_DECODE_INT8 = 0, /* SampleMaterial semantics, integer-exact with the DP4A path */
+  /* The trained float model instead of the int8 blob (ontc_decoder_create_float): features from
+   * the dequantised latent codes in fp32, the fp32 decoder weights, saturated outputs. */
+  ONTC_DECODE_FP32 = 1, /* fp32 arithmetic throughout (CUDA cores) */
+  ONTC_DECODE_BF16 = 2, /* bf16 features, weights and activations; fp32 accumulation (tcgen05) */
+  ONTC_DECODE_FP8 = 3   /* e4m3 with per-layer scales: features x 256, weights at max|W| / 448,
+                           activations at Calibrate's max |activation| / 448; fp32 accumulation */
 };
 
 /* openntc::CalibrationData, openntc_runtime.h:61-67 */
@@ -290,6 +296,14 @@ int ontc_decode(ontc_decoder* dec, const float* d_uv, const int32_t* d_lod, int6
 int ontc_decode_host(ontc_decoder* dec, const float* uv, const int32_t* lod, int64_t n, float* out);
 /* Waits for the decoder's stream; ONTC_CUDA_FAILURE if a decode failed or timed out. */
 int ontc_decoder_status(ontc_decoder* dec);
+
+/* No upstream counterpart: a decoder of a trained context's float model (mode ONTC_DECODE_FP32,
+ * BF16 or FP8): the packed latents of ontc_get_compressed_data with the context's fp32 decoder
+ * weights in place of the int8 blob (FP8: the calibration maxima give the activation scales).
+ * The context must have completed training; the decoder does not keep a reference to it.
+ * ontc_decode and ontc_decode_host work as for the int8 decoder (outputs saturated);
+ * ontc_decode_material and ontc_sample_screen return ONTC_INVALID_STATE for it. */
+int ontc_decoder_create_float(ontc_context* ctx, int32_t mode, void* stream, ontc_decoder** out);
 
 /* MaterialParams (ntc_decode.hlsli:507-522), 72 bytes, filled as DecodeMaterial (:544-603)
  * does: every field starts at DefaultMaterialParams (:524-540) (albedo 0.5, alpha 1,

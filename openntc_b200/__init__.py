@@ -262,6 +262,19 @@ class Decoder:
         self._h = h.value
         self.channels = data.channel_count
 
+    @classmethod
+    def from_context(cls, ctx: "Context", mode: int, stream: int | None = None) -> "Decoder":
+        """A decoder of a trained context's float model: mode _abi.DECODE_FP32 / BF16 / FP8."""
+        self = cls.__new__(cls)
+        self._lib = load()
+        h = C.c_void_p()
+        r = self._lib.ontc_decoder_create_float(ctx.handle, int(mode), stream, C.byref(h))
+        if r != 0:
+            raise RuntimeError(f"ontc_decoder_create_float failed: {Result(r).name}")
+        self._h = h.value
+        self.channels = ctx.get_compressed_data().channel_count
+        return self
+
     def __del__(self):
         if getattr(self, "_h", None):
             self._lib.ontc_decoder_destroy(self._h)

@@ -23,6 +23,7 @@ QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH, QUALITY_ULTRA = range(4)
 MANIFEST_LOADED, TRAIN_IN_PROGRESS, TRAIN_COMPLETE, TRAIN_ERROR = 0, 1, 2, -1
 PRECISION_BF16, PRECISION_FP32 = 0, 1
 DECODE_INT8 = 0  # ONTC_DECODE_INT8: SampleMaterial integer semantics
+DECODE_FP32, DECODE_BF16, DECODE_FP8 = 1, 2, 3  # float-model decoders (ontc_decoder_create_float)
 SCREEN_DISCARD_OUTSIDE = 1  # ONTC_SCREEN_DISCARD_OUTSIDE
 SCREEN_MATERIAL = 2  # ONTC_SCREEN_MATERIAL
 # ontc_material_params: MaterialParams (ntc_decode.hlsli:507-522), 17 floats then `present`
@@ -167,6 +168,7 @@ SIGNATURES = {
     "ontc_decode_host": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "ontc_decoder_status": (C.c_int, [P]),
     "ontc_decode_material": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "ontc_decoder_create_float": (C.c_int, [P, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "ontc_sample_screen": (C.c_int, [P, C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
 }
 

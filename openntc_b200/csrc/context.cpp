@@ -1638,6 +1638,27 @@ void ontc_eval(ontc_context* c, ontc_eval_results* out)
   out->psnr = -10.0 * std::log10(out->mse);
 }
 
+int ontc_decoder_create_float(ontc_context* c, int32_t mode, void* stream, ontc_decoder** out)
+{
+  if (!out) return ONTC_INVALID_STATE;
+  *out = nullptr;
+  if (!c || !c->manifest_loaded || c->train_phase != ONTC_TRAIN_COMPLETE) return ONTC_INVALID_STATE;
+  if (mode != ONTC_DECODE_FP32 && mode != ONTC_DECODE_BF16 && mode != ONTC_DECODE_FP8) return ONTC_INVALID_STATE;
+  ontc_compressed_data cd;
+  ontc_get_compressed_data(c, &cd);
+  int r = ontc_decoder_create(&cd, ONTC_DECODE_INT8, stream, out);
+  if (r != ONTC_SUCCESS) return r;
+  std::vector<float> W(c->nW);
+  if (cudaMemcpy(W.data(), c->W.p, c->nW * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+    r = ONTC_CUDA_FAILURE;
+  if (r == ONTC_SUCCESS) r = ontc::decoder_set_float(*out, mode, W.data(), c->F, c->C, c->caldata);
+  if (r != ONTC_SUCCESS) {
+    ontc_decoder_destroy(*out);
+    *out = nullptr;
+  }
+  return r;
+}
+
 void ontc_eval_decoded(ontc_context* c, ontc_eval_results* out)
 {
   *out = ontc_eval_results{};

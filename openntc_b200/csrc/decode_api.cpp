@@ -5,11 +5,22 @@
 #include <cmath>
 #include <cstring>
 
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include <vector>
+
 #include "kernels.h"
 #include "ontc.h"
 
 struct ontc_decoder {
   int profile = 0;
+  int mode = ONTC_DECODE_INT8;
+  // float-model decoders: the fp32 weights (FP32) or the row-major bf16 / e4m3 tiles (BF16,
+  // FP8) and the FP8 scales
+  float* W32 = nullptr;
+  void* Wq = nullptr;
+  float sx = 1.0f, sw0 = 1.0f, sw1 = 1.0f, swo = 1.0f, sa1 = 1.0f, sa2 = 1.0f;
   cudaStream_t stream = nullptr;
   ontc_constants k = {};
   uint32_t* g0 = nullptr;
@@ -58,6 +69,8 @@ void release(ontc_decoder* d)
   cudaFree(d->g1);
   cudaFree(d->blob);
   cudaFree(d->err);
+  cudaFree(d->W32);
+  cudaFree(d->Wq);
   for (int i = 0; i < ontc_decoder::kPipe; i++) {
     cudaFree(d->uv[i]);
     cudaFree(d->lod[i]);
@@ -155,9 +168,103 @@ int launch(const ontc_decoder* d, const ontc::DecodeArgs& a)
   return ontc::launch_decode(d->profile, a, d->stream) == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
 }
 
+// A list decode on `stream` in the decoder's mode (int8 blob or float model).
+cudaError_t launch_list(const ontc_decoder* d, const float* uv, const int32_t* lod, int64_t n, float* out,
+                        cudaStream_t stream)
+{
+  if (d->mode == ONTC_DECODE_INT8) {
+    ontc::DecodeArgs a = base_args(d);
+    a.uv = uv;
+    a.lod = lod;
+    a.n = n;
+    a.out = out;
+    return ontc::launch_decode(d->profile, a, stream);
+  }
+  ontc::FloatDecodeArgs a;
+  a.g0 = d->g0;
+  a.g1 = d->g1;
+  a.g0_words = d->g0_words;
+  a.g1_words = d->g1_words;
+  a.k = d->k;
+  a.W = d->W32;
+  a.Wq = d->Wq;
+  a.sx = d->sx;
+  a.sw0 = d->sw0;
+  a.sw1 = d->sw1;
+  a.swo = d->swo;
+  a.sa1 = d->sa1;
+  a.sa2 = d->sa2;
+  a.uv = uv;
+  a.lod = lod;
+  a.n = n;
+  a.out = out;
+  a.err = d->err;
+  return ontc::launch_decode_float(d->profile, d->mode, a, stream);
+}
+
+float max_abs(const float* w, int n)
+{
+  float m = 0.0f;
+  for (int i = 0; i < n; i++) m = std::max(m, std::fabs(w[i]));
+  return m;
+}
+
 }  // namespace
 
 namespace ontc {
+
+int decoder_set_float(ontc_decoder* d, int mode, const float* W, int F, int C, const ontc_calibration& cal)
+{
+  if (!d || !W || (mode != ONTC_DECODE_FP32 && mode != ONTC_DECODE_BF16 && mode != ONTC_DECODE_FP8))
+    return ONTC_INVALID_STATE;
+  const int H = 64, nW = H * F + H * H + 16 * H;
+  // Wout rows past the channel count are not trained (libopenntc.cpp:722-754): zero them
+  std::vector<float> w(W, W + nW);
+  for (int i = wo_off(F) + C * H; i < nW; i++) w[i] = 0.0f;
+  d->mode = mode;
+  if (mode == ONTC_DECODE_FP32) {
+    if (cudaMalloc(&d->W32, nW * sizeof(float)) != cudaSuccess) return ONTC_ALLOCATION_FAILURE;
+    return cudaMemcpy(d->W32, w.data(), nW * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess
+               ? ONTC_SUCCESS
+               : ONTC_CUDA_FAILURE;
+  }
+  // row-major W0 [64][Kp] (zero past F) | W1 [64][64] | Wout [16][64]
+  const int Kp = float_decode_kp(d->profile);
+  if (Kp < F) return ONTC_INVALID_STATE;
+  std::vector<float> rows((size_t)H * Kp + H * H + 16 * H, 0.0f);
+  for (int r = 0; r < H; r++)
+    for (int c = 0; c < F; c++) rows[(size_t)r * Kp + c] = w[(size_t)r * F + c];
+  std::copy(w.begin() + w1_off(F), w.end(), rows.begin() + (size_t)H * Kp);
+  const float* W0 = rows.data();
+  const float* W1 = W0 + H * Kp;
+  const float* Wo = W1 + H * H;
+  std::vector<uint8_t> bytes;
+  if (mode == ONTC_DECODE_BF16) {
+    bytes.resize(rows.size() * 2);
+    for (size_t i = 0; i < rows.size(); i++) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(rows[i]);
+      memcpy(&bytes[2 * i], &b, 2);
+    }
+  } else {
+    // per-layer scales: weights at max|W| / 448 (e4m3's largest finite value), features x 256
+    // (they lie in [-1, 1]), activations at Calibrate's max |hardgelu| / 448
+    auto scale = [](float m) { return m > 0.0f ? m / 448.0f : 1.0f; };
+    d->sw0 = scale(max_abs(W0, H * Kp));
+    d->sw1 = scale(max_abs(W1, H * H));
+    d->swo = scale(max_abs(Wo, 16 * H));
+    d->sx = 1.0f / 256.0f;
+    d->sa1 = scale(cal.max_abs_a1);
+    d->sa2 = scale(cal.max_abs_a2);
+    bytes.resize(rows.size());
+    for (size_t i = 0; i < rows.size(); i++) {
+      const float s = i < (size_t)H * Kp ? d->sw0 : (i < (size_t)H * Kp + H * H ? d->sw1 : d->swo);
+      bytes[i] = (uint8_t)__nv_cvt_float_to_fp8(rows[i] / s, __NV_SATFINITE, __NV_E4M3);
+    }
+  }
+  if (cudaMalloc(&d->Wq, bytes.size()) != cudaSuccess) return ONTC_ALLOCATION_FAILURE;
+  return cudaMemcpy(d->Wq, bytes.data(), bytes.size(), cudaMemcpyHostToDevice) == cudaSuccess ? ONTC_SUCCESS
+                                                                                             : ONTC_CUDA_FAILURE;
+}
 
 int decoder_set_weights(ontc_decoder* d, const uint8_t* blob, size_t size, float s_a1, float s_a2)
 {
@@ -234,19 +341,14 @@ void ontc_decoder_destroy(ontc_decoder* d)
 int ontc_decode(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out)
 {
   if (!d || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_out))) return ONTC_INVALID_STATE;
-  ontc::DecodeArgs a = base_args(d);
-  a.uv = d_uv;
-  a.lod = d_lod;
-  a.n = n;
-  a.out = d_out;
-  return launch(d, a);
+  return launch_list(d, d_uv, d_lod, n, d_out, d->stream) == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
 }
 
 int ontc_decode_material(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n,
                          ontc_material_params* d_params)
 {
   if (!d || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_params))) return ONTC_INVALID_STATE;
-  if (reinterpret_cast<uintptr_t>(d_params) % 8 != 0) return ONTC_INVALID_STATE;
+  if (d->mode != ONTC_DECODE_INT8 || reinterpret_cast<uintptr_t>(d_params) % 8 != 0) return ONTC_INVALID_STATE;
   ontc::DecodeArgs a = base_args(d);
   a.uv = d_uv;
   a.lod = d_lod;
@@ -259,7 +361,8 @@ int ontc_decode_material(ontc_decoder* d, const float* d_uv, const int32_t* d_lo
 int ontc_sample_screen(ontc_decoder* d, const float* d_uv, int32_t width, int32_t height, float noise_frame,
                        int32_t flags, void* d_out)
 {
-  if (!d || width < 0 || height < 0 || (flags & ~(ONTC_SCREEN_DISCARD_OUTSIDE | ONTC_SCREEN_MATERIAL)))
+  if (!d || d->mode != ONTC_DECODE_INT8 || width < 0 || height < 0 ||
+      (flags & ~(ONTC_SCREEN_DISCARD_OUTSIDE | ONTC_SCREEN_MATERIAL)))
     return ONTC_INVALID_STATE;
   if (width == 0 || height == 0) return ONTC_SUCCESS;
   if (!d_uv || !d_out || reinterpret_cast<uintptr_t>(d_uv) % 8 != 0 ||
@@ -306,14 +409,7 @@ int ontc_decode_host(ontc_decoder* d, const float* uv, const int32_t* lod, int64
     const int64_t m = std::min<int64_t>(ontc_decoder::kChunk, n - j0);
     e = cudaMemcpyAsync(d->uv[p], uv + 2 * j0, (size_t)m * 2 * sizeof(float), cudaMemcpyHostToDevice, d->pipe[p]);
     if (!e) e = cudaMemcpyAsync(d->lod[p], lod + j0, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, d->pipe[p]);
-    if (!e) {
-      ontc::DecodeArgs a = base_args(d);
-      a.uv = d->uv[p];
-      a.lod = d->lod[p];
-      a.n = m;
-      a.out = d->out[p];
-      e = ontc::launch_decode(d->profile, a, d->pipe[p]);
-    }
+    if (!e) e = launch_list(d, d->uv[p], d->lod[p], m, d->out[p], d->pipe[p]);
     if (!e)
       e = cudaMemcpyAsync(out + j0 * C, d->out[p], (size_t)m * C * sizeof(float), cudaMemcpyDeviceToHost, d->pipe[p]);
   }

@@ -38,6 +38,32 @@ struct DecodeArgs {
   uint32_t material_present = 0;
 };
 cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
+// The float-model decoders (decode_float.cu): the trained fp32 decoder weights evaluated on the
+// dequantised latent codes.  mode: ONTC_DECODE_FP32 (fp32 CUDA-core arithmetic), BF16
+// (tcgen05 bf16, fp32 accumulate), FP8 (tcgen05 e4m3 with per-layer scales, fp32 accumulate).
+struct FloatDecodeArgs {
+  const uint32_t* g0;
+  const uint32_t* g1;
+  uint32_t g0_words, g1_words;
+  ontc_constants k;
+  const float* W;    // FP32: W0 [64][F] | W1 [64][64] | Wout [16][64] (the training layout)
+  const void* Wq;    // BF16 / FP8: W0 [64][Kp] | W1 [64][64] | Wout [16][64] elements, row-major
+  float sx = 1.0f;   // FP8: feature, weight and activation scales (value = code x scale)
+  float sw0 = 1.0f, sw1 = 1.0f, swo = 1.0f, sa1 = 1.0f, sa2 = 1.0f;
+  const float* uv;
+  const int32_t* lod;
+  int64_t n;
+  float* out;        // [n][k.channel_count], saturated
+  int* err;          // set to 1 when a bounded wait gave up
+};
+cudaError_t launch_decode_float(int profile, int mode, const FloatDecodeArgs& args, cudaStream_t stream);
+// Kp of a profile's float decoder (the training feature width rounded up to 32)
+int float_decode_kp(int profile);
+
+// Turns a decoder into a float-model one (mode ONTC_DECODE_FP32 / BF16 / FP8) with the fp32
+// weights W (training layout, feature width F), C output channels and the calibration maxima
+// (FP8 activation scales).  ONTC_* status.
+int decoder_set_float(ontc_decoder* dec, int mode, const float* W, int F, int C, const ontc_calibration& cal);
 // Replaces a decoder's int8 blob and activation scales (same layout and shapes); waits for its
 // stream first.  ONTC_* status.
 int decoder_set_weights(ontc_decoder* dec, const uint8_t* blob, size_t size, float s_a1, float s_a2);
