@@ -30,9 +30,11 @@ def test_no_gradient_left_outside_footprints(materials):
             assert not g.any(), (name, l, int(np.count_nonzero(g)))
 
 
-def _run(manifest, mode, precision, steps):
-    ctx = H.new_context(ont.Profile.Bpp_0_5, manifest, min_dim=1024, grids=1, steps=steps, precision=precision,
+def _run(manifest, mode, precision, steps, pieces=(), grids=1):
+    ctx = H.new_context(ont.Profile.Bpp_0_5, manifest, min_dim=1024, grids=grids, steps=steps, precision=precision,
                         latent_adam=mode)
+    for n in pieces:  # ontc_train calls of these sizes first (each ends a chunk)
+        assert ctx.train(n).result == 0
     p = ctx.train_until_complete()
     assert p.phase == ont.TrainPhase.TrainComplete and p.result == 0
     sh = H.shape(ctx)
@@ -54,6 +56,26 @@ def test_deferred_matches_dense(materials, precision):
     # Float atomics make every run differ slightly, most on small levels trained with whole-mip
     # tiles; a missed or doubled replay would move a moment by a factor of beta^k, i.e. by
     # tens of percent, far beyond this bound.
+    for key in a:
+        spread = np.abs(b[key] - a[key]).max()
+        diff = np.abs(d[key] - a[key]).max()
+        scale = np.abs(a[key]).max()
+        assert diff <= max(8 * spread, 5e-3 * scale), (key, diff, spread, scale)
+    del ca, cb, cd
+
+
+def test_deferred_in_irregular_calls_matches_dense(materials):
+    """The same comparison with the deferred run trained in calls of 1, 7, 13, 2, 64, 9 and 1
+    steps before the rest: every call ends a chunk, so the two-stream lookahead (the next step's
+    catch-up beside this step's tile kernel) is cut at many points, and the side stream drains
+    before each call returns.  Four tiles per step, so footprints overlap from step to step."""
+    manifest = materials(1024, 8, 9)
+    psnr_a, a, ca = _run(manifest, ont.LatentAdam.DENSE, ont.Precision.BF16, 150, grids=4)
+    psnr_b, b, cb = _run(manifest, ont.LatentAdam.DENSE, ont.Precision.BF16, 150, grids=4)
+    psnr_d, d, cd = _run(manifest, ont.LatentAdam.DEFERRED, ont.Precision.BF16, 150,
+                         pieces=(1, 7, 13, 2, 64, 9, 1), grids=4)
+    print(f"PSNR dense {psnr_a:.4f} / {psnr_b:.4f}, deferred in pieces {psnr_d:.4f} dB")
+    assert abs(psnr_d - psnr_a) < max(4 * abs(psnr_b - psnr_a), 0.02)
     for key in a:
         spread = np.abs(b[key] - a[key]).max()
         diff = np.abs(d[key] - a[key]).max()
