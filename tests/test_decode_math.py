@@ -1,4 +1,4 @@
-"""Arithmetic claims the decode kernel rests on, checked on the CPU."""
+"""Arithmetic claims the kernels rest on, checked on the CPU."""
 import os
 
 
@@ -28,3 +28,14 @@ def test_stochastic_filter_semantics(oracle):
     assert abs(lod_ab2.mean() - (2.3 + 4 - 3)) < 1e-3  # log2(16 * 2^2.3 / 8)
     uv3, _, keep3, _, _ = oracle.screen_filter(img * 8, dim, 11, 0.0, True)  # uv up to 8: discarded
     assert 0 < keep3.sum() < len(keep3)
+
+
+def test_box_index_quotient_by_reciprocal_is_exact():
+    """The tile kernel's box loops take v / d as floor((v + 0.5) * RN(1/d)) in fp32 (div_small):
+    exact for every v < 4096 and 1 <= d <= 512, which covers the staged-box item and cell indices."""
+    import numpy as np
+    v = np.arange(0, 4096, dtype=np.int64)
+    for d in range(1, 513):
+        inv = np.float32(1.0) / np.float32(d)
+        q = np.floor((v.astype(np.float32) + np.float32(0.5)) * inv).astype(np.int64)
+        assert np.array_equal(q, v // d), d
