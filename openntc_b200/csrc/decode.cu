@@ -216,32 +216,74 @@ __device__ __forceinline__ void st16(uint8_t* base, int r, int c0, int cols, uin
 // 16 accumulator columns of this thread's row -> 16 requantised activations (4 words).  The
 // arithmetic of hg_hlsl and q8_bits, two columns at a time on packed fp32 pairs (each lane
 // rounds exactly as the scalar operation).
+//
+// kFast (for 1.6e-5 <= rcp <= 600) forms the same bytes with fewer select / compare steps:
+// hardgelu as mid(max(min(x, 1.5), -1.5)) + (x - min(x, 1.5)), where the remainder is exact
+// for |x| < 2^23 and mid(1.5) = 1.5, so the sum is x above 1.5 and mid below (equal to the
+// select form for every float with |x| < 2^23, checked exhaustively on the CPU); from 2^23 up
+// both forms give at least 2^23, which saturates to 127 at rcp >= 1.6e-5.  hardgelu is at
+// least -0.1875, so at rcp <= 600 the scaled value stays above -113 and the lower clamp never
+// binds.
+template <bool kFast>
 __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restrict__ scale, float rcp, uint32_t* out)
 {
   float acc[16];
   ptx::ld16(taddr, acc);
   ptx::ld_wait();
   const float2 third = make_float2(1.0f / 3.0f, 1.0f / 3.0f), m3 = make_float2(-3.0f, -3.0f);
-  const float2 h15 = make_float2(1.5f, 1.5f), r2 = make_float2(rcp, rcp);
+  const float2 h15 = make_float2(1.5f, 1.5f), r2 = make_float2(rcp, rcp), m1 = make_float2(-1.0f, -1.0f);
   const float2 magic = make_float2(12582912.0f, 12582912.0f);
   uint32_t b[16];
 #pragma unroll
   for (int j = 0; j < 16; j += 2) {
     const float2 x = ptx::mul2(make_float2((float)__float_as_int(acc[j]), (float)__float_as_int(acc[j + 1])),
                                *reinterpret_cast<const float2*>(scale + j));
-    const float2 c = make_float2(fmaxf(x.x, -1.5f), fmaxf(x.y, -1.5f));
-    const float2 q = ptx::mul2(c, third);                    // div3: RN(c * RN(1/3)),
-    const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);  // corrected by the exact remainder
-    const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
-    const float2 hg = make_float2(x.x < 1.5f ? mid.x : x.x, x.y < 1.5f ? mid.y : x.y);
-    float2 f = ptx::mul2(hg, r2);
-    f = make_float2(fminf(fmaxf(f.x, -128.0f), 127.0f), fminf(fmaxf(f.y, -128.0f), 127.0f));
+    float2 f;
+    if constexpr (kFast) {
+      const float2 hi = make_float2(fminf(x.x, 1.5f), fminf(x.y, 1.5f));
+      const float2 c = make_float2(fmaxf(hi.x, -1.5f), fmaxf(hi.y, -1.5f));
+      const float2 q = ptx::mul2(c, third);
+      const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);
+      const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
+      const float2 hg = ptx::add2(mid, ptx::fma2(hi, m1, x));
+      f = ptx::mul2(hg, r2);
+      f = make_float2(fminf(f.x, 127.0f), fminf(f.y, 127.0f));
+    } else {
+      const float2 c = make_float2(fmaxf(x.x, -1.5f), fmaxf(x.y, -1.5f));
+      const float2 q = ptx::mul2(c, third);                    // div3: RN(c * RN(1/3)),
+      const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);  // corrected by the exact remainder
+      const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
+      const float2 hg = make_float2(x.x < 1.5f ? mid.x : x.x, x.y < 1.5f ? mid.y : x.y);
+      f = ptx::mul2(hg, r2);
+      f = make_float2(fminf(fmaxf(f.x, -128.0f), 127.0f), fminf(fmaxf(f.y, -128.0f), 127.0f));
+    }
     const float2 k = ptx::add2(f, magic);
     b[j] = __float_as_uint(k.x);
     b[j + 1] = __float_as_uint(k.y);
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) out[i] = pack4(b[4 * i], b[4 * i + 1], b[4 * i + 2], b[4 * i + 3]);
+}
+
+// One hidden layer's 64 columns of this thread's row, requantised into the next operand tile.
+__device__ __forceinline__ void requant_row(uint32_t taddr, const float* __restrict__ scale, float rcp, bool fast,
+                                            uint8_t* X, int row)
+{
+  if (fast) {
+#pragma unroll
+    for (int c = 0; c < kHid; c += 16) {
+      uint32_t q[4];
+      requant16<true>(taddr + c, scale + c, rcp, q);
+      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < kHid; c += 16) {
+      uint32_t q[4];
+      requant16<false>(taddr + c, scale + c, rcp, q);
+      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
+    }
+  }
 }
 
 template <class SH>
@@ -384,6 +426,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   const bool issuer = row == 0, poller = (row >> 5) == 0;
   const int C = A.k.channel_count;
   const float rcp1 = A.k.rcp_s_a1, rcp2 = A.k.rcp_s_a2;
+  const bool fast1 = rcp1 >= 1.6e-5f && rcp1 <= 600.0f, fast2 = rcp2 >= 1.6e-5f && rcp2 <= 600.0f;
 
   constexpr uint32_t I_L01 = ptx::idesc_s8(128, kHid, false, false);
   constexpr uint32_t I_L2 = ptx::idesc_s8(128, kOutRows, false, false);
@@ -439,12 +482,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a0 -> A (over X)
-#pragma unroll
-    for (int c = 0; c < kHid; c += 16) {
-      uint32_t q[4];
-      requant16(lwin + c, s0 + c, rcp1, q);
-      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
-    }
+    requant_row(lwin, s0, rcp1, fast1, X, row);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
@@ -455,12 +493,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a1 -> A
-#pragma unroll
-    for (int c = 0; c < kHid; c += 16) {
-      uint32_t q[4];
-      requant16(lwin + c, s1 + c, rcp2, q);
-      st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
-    }
+    requant_row(lwin, s1, rcp2, fast2, X, row);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();

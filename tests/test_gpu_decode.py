@@ -122,6 +122,24 @@ def test_int8_decode_tracks_the_float_model(trained, oracle):
     assert err.mean() < 0.02 and err.max() < 0.25, (err.mean(), err.max())
 
 
+@pytest.mark.parametrize("s_a", [(1e-3, None), (None, 1e5), (1e-3, 1e5)])
+def test_decode_extreme_activation_scales(trained, oracle, s_a):
+    """Activation scales whose reciprocals lie outside [1.6e-5, 600] (a hidden layer whose
+    activations nearly all saturate at -128 or at 127) take the requantisation with both clamps
+    and the select form of hardgelu; trained scales take the shorter form.  Both match the
+    oracle bit for bit, alone and mixed across the two hidden layers."""
+    ctx = trained[ont.Profile.Bpp_1_0]
+    cd = type(ctx.get_compressed_data()).from_buffer_copy(ctx.get_compressed_data())
+    if s_a[0] is not None:
+        cd.caldata.s_a1 = s_a[0]
+    if s_a[1] is not None:
+        cd.caldata.s_a2 = s_a[1]
+    uv, lod = samples(9000 + 11, cd.mip_count, 23)
+    got = ont.Decoder(cd).decode_host(uv, lod)
+    want = oracle_decode(oracle, cd, uv, lod)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 def test_decoder_rejects_mismatched_data(trained):
     cd = ctx_cd = trained[ont.Profile.Bpp_0_2].get_compressed_data()
     lib = ont.load()
