@@ -118,9 +118,56 @@ __device__ __forceinline__ void put_byte(uint32_t* w, int f, int v)
   w[f >> 2] |= ((uint32_t)v & 0xFFu) << (8 * (f & 3));
 }
 
+// One triangle-wave feature byte (ntc_decode.hlsli:300-330): wave p (period 8 >> p) of texel
+// coordinate c, phase h.  For an integer-valued |c| < 2^22 every step is exact (c + 0.5 and the
+// quarter-period phase are representable, the period is a power of two), so the byte depends
+// only on c mod 8: the decode reads it from a table built with this function.
+__device__ __forceinline__ int tri_q8(float c, int p, int h)
+{
+  const float P = (float)(8 >> p), rP = 1.0f / P;  // P = 8, 4, 2: dividing = exact scaling
+  const float ph = h == 0 ? 0.0f : __fmul_rn(0.25f, P);
+  const float t = __fmul_rn(__fadd_rn(__fadd_rn(c, 0.5f), ph), rP);
+  const float pe = __fsub_rn(1.0f, __fmul_rn(4.0f, fabsf(__fsub_rn(__fsub_rn(t, floorf(t)), 0.5f))));
+  return q8(__fmul_rn(pe, 128.0f));
+}
+
+// The normalised-lod feature byte of lod l.
+__device__ __forceinline__ int lod_q8(int l, int mip_count)
+{
+  return q8(__fmul_rn(__fdiv_rn((float)l, (float)(mip_count - 1)), 128.0f));
+}
+
+// Per-CTA tables of the features that depend only on (texel coordinate mod 8) and on lod:
+// tri[a][p][m] holds wave p's two phase bytes of axis a (x: bytes 0-1, y: bytes 2-3 of the
+// feature word p) at coordinate m; lodb[l] the lod byte.
+struct FeatureTables {
+  uint32_t tri[2][3][8];
+  uint32_t lodb[32];
+};
+
+__device__ __forceinline__ void build_feature_tables(FeatureTables& T, int mip_count, int tid)
+{
+  if (tid < 48) {
+    const int a = tid / 24, p = (tid / 8) % 3, m = tid & 7;
+    const uint32_t v = ((uint32_t)tri_q8((float)m, p, 0) & 0xFFu) | (((uint32_t)tri_q8((float)m, p, 1) & 0xFFu) << 8);
+    T.tri[a][p][m] = v << (16 * a);
+  } else if (tid < 80) {
+    T.lodb[tid - 48] = (uint32_t)lod_q8(tid - 48, mip_count) & 0xFFu;
+  }
+}
+
+// Four feature bytes starting at byte f (a compile-time offset) into w[].
+__device__ __forceinline__ void put_word(uint32_t* w, int f, uint32_t v)
+{
+  const int sh = 8 * (f & 3);
+  w[f >> 2] |= v << sh;
+  if (sh != 0) w[(f >> 2) + 1] |= v >> (32 - sh);
+}
+
 // GetFeaturesPacked (ntc_decode.hlsli:196-342) for one sample -> Kp signed bytes in w[].
 template <class SH>
-__device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, int lod, uint32_t* w)
+__device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, int lod, uint32_t* w,
+                                         const FeatureTables& T)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, B0 = SH::B0, B1 = SH::B1;
   const ontc_constants& k = A.k;
@@ -188,21 +235,20 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
   {
     const float cdim = (float)(k.dim >> lod);
     const float tcx = floorf(__fmul_rn(u, cdim)), tcy = floorf(__fmul_rn(v, cdim));
+    constexpr int base = 4 * C0 + C1;
+    if (fabsf(tcx) < 4194304.0f && fabsf(tcy) < 4194304.0f) {
+      const int mx = (int)tcx & 7, my = (int)tcy & 7;  // floor-mod, negative coordinates too
 #pragma unroll
-    for (int p = 0; p < 3; p++)
+      for (int p = 0; p < 3; p++) put_word(w, base + 4 * p, T.tri[0][p][mx] | T.tri[1][p][my]);
+    } else {
 #pragma unroll
-      for (int a = 0; a < 2; a++)
+      for (int p = 0; p < 3; p++)
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const float P = (float)(8 >> p), rP = 1.0f / P;  // P = 8, 4, 2: dividing = exact scaling
-          const float c = a == 0 ? tcx : tcy;
-          const float ph = h == 0 ? 0.0f : __fmul_rn(0.25f, P);
-          const float t = __fmul_rn(__fadd_rn(__fadd_rn(c, 0.5f), ph), rP);
-          const float pe = __fsub_rn(1.0f, __fmul_rn(4.0f, fabsf(__fsub_rn(__fsub_rn(t, floorf(t)), 0.5f))));
-          put_byte(w, 4 * C0 + C1 + p * 4 + a * 2 + h, q8(__fmul_rn(pe, 128.0f)));
-        }
-    const float nl = __fdiv_rn((float)lod, (float)(k.mip_count - 1));
-    put_byte(w, 4 * C0 + C1 + 12, q8(__fmul_rn(nl, 128.0f)));
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) put_byte(w, base + p * 4 + a * 2 + h, tri_q8(a == 0 ? tcx : tcy, p, h));
+    }
+    put_byte(w, base + 12, lod < 32 ? (int)T.lodb[lod] : lod_q8(lod, k.mip_count));
   }
 }
 
@@ -396,6 +442,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   __shared__ uint32_t tmem_base_s;
   __shared__ int fail_s;
   __shared__ __align__(16) float s0[kHid], s1[kHid], so[kOutRows];  // read as float2 pairs
+  __shared__ FeatureTables tables_s;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -414,6 +461,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   }
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, 64 * kGroups);  // a power of two: 512
   load_decoder<SH>(A.blob, sW0, sW1, sWo, s0, s1, so);
+  build_feature_tables(tables_s, A.k.mip_count, tid);
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
@@ -464,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
           v = uv.y;
           lod = A.lod[i];
         }
-        features<SH>(A, u, v, lod, w);
+        features<SH>(A, u, v, lod, w, tables_s);
       } else {
 #pragma unroll
         for (int j = 0; j < Kp / 4; j++) w[j] = 0u;

@@ -140,6 +140,23 @@ def test_decode_extreme_activation_scales(trained, oracle, s_a):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
+def test_decode_uv_outside_the_unit_square(trained, oracle):
+    """Coordinates outside [0, 1): the triangle-wave features come from per-CTA tables indexed
+    by texel coordinate mod 8 while |floor(u * dim)| < 2^22 (negative ones too) and from the
+    float formula beyond; both match the oracle bit for bit."""
+    ctx = trained[ont.Profile.Bpp_2_25]
+    cd = ctx.get_compressed_data()
+    rng = np.random.default_rng(31)
+    n = 6000
+    near = rng.uniform(-3.0, 3.0, (n, 2))
+    far = rng.uniform(16384.0, 40000.0, (n, 2)) * rng.choice([-1.0, 1.0], (n, 2))
+    uv = np.concatenate([near, far]).astype(np.float32)
+    lod = rng.integers(0, cd.mip_count, 2 * n).astype(np.int32)
+    got = ont.Decoder(cd).decode_host(uv, lod)
+    want = oracle_decode(oracle, cd, uv, lod)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 def test_decoder_rejects_mismatched_data(trained):
     cd = ctx_cd = trained[ont.Profile.Bpp_0_2].get_compressed_data()
     lib = ont.load()
