@@ -403,7 +403,10 @@ const char* ontc_version(void);
  * 2048^2 x 1).  ch 1..4.  Calls whose executions overlap (different streams, or host threads
  * without ordering) race on that array: issue them on one stream or order them.  The first
  * call on each device looks the array up (cudaGetSymbolAddress); make it before any stream
- * capture on that device.  Returns when the work is enqueued. */
+ * capture on that device.  The array is part of the library's device code, so loading
+ * libontc reserves its 8 MiB on every device the library runs on, whether or not this entry
+ * point is called.  Returns when the work is enqueued; ONTC_CUDA_FAILURE reports a launch
+ * error of this call or a sticky error of an earlier fault on the device. */
 #define ONTC_NOALLOC_SCRATCH_FLOATS 2097152
 int ontc_lanczos_down_noalloc(const uint8_t* d_src, int32_t dim, int32_t ch, uint8_t* d_dst, void* stream);
 

@@ -87,6 +87,42 @@ int ontc_debug_disjoint_cover(const int32_t* in, int32_t n, int32_t* out, int32_
 int ontc_debug_cover_op(const int32_t* a, int32_t na, const int32_t* b, int32_t nb, int32_t op, int32_t* out,
                         int32_t cap);
 
+/* Test mode of the BF16 (tcgen05) training tile kernel: each feature gradient is replaced by
+ * n * 2^-24, n = clamp(rint(g * 2^24), -15, 15), before it is scattered into the latent
+ * gradients.  Every latent gradient is then an exactly representable sum, so the float atomics
+ * give the same bits in any order.  The decoder is held fixed in this mode (its learning rate
+ * is zero): the two tile groups of a CTA add their weight-gradient products to shared TMEM
+ * accumulators in arrival order, so the decoder gradient is not bit-reproducible.  Two runs
+ * from the same state then leave bit-identical latents, latent moments and decoder weights
+ * (used to compare the deferred latent optimiser with the dense one bit for bit).  Takes
+ * effect for steps drawn after the call. */
+int ontc_debug_exact_gradients(ontc_context* ctx, int32_t enable);
+
+/* Training completion (upstream libopenntc.cpp:799-876: pack the latents, Calibrate,
+ * QuantizeWeights into the decoder blob) on the context's current state, without a training
+ * step: lets a test load a state (ontc_debug_tensor) and compare the artefacts with another
+ * implementation's.  s_a: NULL, or {s_a1, s_a2} to build the blob with these activation scales
+ * instead of the calibrated ones (the calibration maxima are still computed and reported).
+ * The context is complete afterwards. */
+int ontc_debug_complete(ontc_context* ctx, const float* s_a);
+
+/* The int8 decoder's feature bytes (GetFeaturesPacked, ntc_decode.hlsli:196-342) for n samples
+ * on the device: out[n][96] int8, the first Kp (64 or 96) bytes of each row written by the
+ * decode kernel itself, the rest zero.  Int8 decoders only. */
+int ontc_debug_decode_features(ontc_decoder* dec, const float* d_uv, const int32_t* d_lod, int64_t n, int8_t* d_out);
+
+/* Failure injection on the host: the n-th device allocation the library's contexts make from
+ * now on (n >= 1) fails as an out-of-memory cudaMalloc would, without calling it; n = 0 disarms.
+ * Returns how many such allocations were made before the call, so a test can count the
+ * allocation points of a sequence of calls and fail each one in turn.  Process-wide. */
+int64_t ontc_debug_fail_device_alloc(int64_t n);
+
+/* The manifest image loader on its own (host code, no device): the file at `path` as RGBA8,
+ * the expansion upstream's stbi_load(path, .., 4) gives (libopenntc.cpp:1302).  Writes the
+ * size; rgba (NULL: size only) receives width * height * 4 bytes.  ONTC_FILE_NOT_FOUND when the
+ * file cannot be read or decoded (upstream's LoadManifest result for such a file). */
+int ontc_debug_load_image(const char* path, int32_t* width, int32_t* height, uint8_t* rgba);
+
 /* The bounded wait of the tcgen05 kernels, exercised: one GPU thread waits `polls` (1..1000)
  * suspended polls of up to ~100 us on a barrier nothing arrives at.  Returns ONTC_CUDA_FAILURE
  * when the wait gave up and reported it (the expected outcome), ONTC_INVALID_STATE otherwise. */

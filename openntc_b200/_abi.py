@@ -161,6 +161,11 @@ SIGNATURES = {
     "ontc_debug_cover_op": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]),
     "ontc_lanczos_down_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "ontc_debug_wait_timeout": (C.c_int, [C.c_int32]),
+    "ontc_debug_exact_gradients": (C.c_int, [P, C.c_int32]),
+    "ontc_debug_fail_device_alloc": (C.c_int64, [C.c_int64]),
+    "ontc_debug_load_image": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "ontc_debug_complete": (C.c_int, [P, C.c_void_p]),
+    "ontc_debug_decode_features": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "ontc_train_batch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TrainProgress)]),
     "ontc_decoder_create": (C.c_int, [C.POINTER(CompressedData), C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "ontc_decoder_destroy": (None, [P]),

@@ -41,6 +41,7 @@ struct StepRec {
   int32_t gstep;        // step index within the level (grid_batch_i_ before the step)
   int32_t gfloor;       // deferred optimiser: every latent of the level has had >= gfloor steps
   int32_t sweep_from;   // host only: floor before the level sweep that precedes this step, or -1
+  int32_t exact_grad;   // test mode: latent gradients as exactly-summable dyadic values (see train_tc.cu)
 };
 
 // Latent cells a step can touch, as DISJOINT rectangles per pyramid: the union of every

@@ -15,6 +15,7 @@
 // on one stream, the step's draws uploaded in batches ahead of time, no host sync per step,
 // quantisation noise generated at the touched latents only, FP64 loss and PSNR sums.
 #include <algorithm>
+#include <atomic>
 #include <bit>
 #include <cmath>
 #include <cstdio>
@@ -38,6 +39,11 @@ using namespace ontc;
 
 namespace {
 
+// Device allocations made through DBuf so far, and the one to fail (ontc_debug_fail_device_alloc;
+// 0: none): a host-side stand-in for an out-of-memory cudaMalloc.
+std::atomic<int64_t> g_dev_allocs{0};
+std::atomic<int64_t> g_fail_alloc{0};
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -47,6 +53,11 @@ struct DBuf {
     release();
     n = count;
     if (count == 0) return cudaSuccess;
+    const int64_t k = ++g_dev_allocs;
+    if (k == g_fail_alloc.load()) {
+      n = 0;
+      return cudaErrorMemoryAllocation;
+    }
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
@@ -197,6 +208,7 @@ struct ontc_context {
   int32_t noise_mode = ONTC_NOISE_COUNTER;
   int32_t optimizer = ONTC_LATENT_ADAM_DEFERRED;
   int32_t calibration = ONTC_CALIBRATION_UPSTREAM;
+  bool exact_grad = false;  // ontc_debug_exact_gradients
   int32_t upd_count[ONTC_MAX_LEVELS] = {};  // level steps with a latent update (before the lock)
   int32_t swept[ONTC_MAX_LEVELS] = {};      // every cell of the level has received this many
   int32_t lock_from[ONTC_MAX_LEVELS] = {}, lock_to[ONTC_MAX_LEVELS] = {};  // sweeps at the lock
@@ -591,9 +603,9 @@ StepRec full_mip_rec(const ontc_context* c, int mip)
   return s;
 }
 
+// Releases everything a manifest holds, also the buffers of a load that failed part way.
 void unload(ontc_context* c)
 {
-  if (!c->manifest_loaded) return;
   for (int g = 0; g < 2; g++)
     for (int k = 0; k < 4; k++)
       for (int l = 0; l < ONTC_MAX_LEVELS; l++) c->lat[g][k][l].release();
@@ -956,8 +968,19 @@ int ontc_init(ontc_context* c, int32_t profile, void* stream)
   }
   if (c->W.alloc(c->nW) || c->Wm.alloc(c->nW) || c->Wv.alloc(c->nW) || c->dWpart.alloc((size_t)c->max_grid * c->nW) ||
       c->loss_part.alloc(c->max_grid) || c->calib.alloc(2) || c->eval_sums.alloc(ONTC_MAX_MIPS) ||
-      c->aux_steps.alloc(ONTC_MAX_MIPS) || c->tc_error.alloc(4) || !ensure_host_steps(c, 1024))
+      c->aux_steps.alloc(ONTC_MAX_MIPS) || c->tc_error.alloc(4) || !ensure_host_steps(c, 1024)) {
+    // a failed Init holds nothing: it can be retried, or the context destroyed
+    for (auto* b : {&c->W, &c->Wm, &c->Wv, &c->dWpart}) b->release();
+    c->loss_part.release();
+    c->calib.release();
+    c->aux_steps.release();
+    c->tc_error.release();
+    c->eval_sums.release();
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = nullptr;
+    c->own_stream = false;
     return ONTC_ALLOCATION_FAILURE;
+  }
   cudaMemset(c->W.p, 0, c->nW * sizeof(float));
   cudaMemset(c->tc_error.p, 0, 4 * sizeof(int));
   const size_t dec = (size_t)kHidden * c->Fp + kHidden * kHidden + kOutPad * kHidden + kHidden * 4 + kHidden * 4 +
@@ -1035,6 +1058,9 @@ int ontc_load_manifest(ontc_context* c, const char* path)
       s.vflip = vf ? vf->as_bool() : false;
       s.sem = sem;
       s.nch = ontc_channel_count_for_semantic(sem);
+      // an unknown semantic name has no channel count (upstream carries -1 on into its totals,
+      // allocations and launches when valid sources make the total positive): rejected here
+      if (s.nch < 1) return ONTC_INVALID_MANIFEST;
       for (int i = 0; i < 4; i++) {
         int ch = -1;
         if (i < s.nch) ch = chs[i] == 'R' ? 0 : chs[i] == 'G' ? 1 : chs[i] == 'B' ? 2 : 3;
@@ -1177,7 +1203,7 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
 {
   if (!c->manifest_loaded ||
       (c->train_phase != ONTC_MANIFEST_LOADED && c->train_phase != ONTC_TRAIN_COMPLETE &&
-       c->train_phase != ONTC_TRAIN_IN_PROGRESS)) {
+       c->train_phase != ONTC_TRAIN_IN_PROGRESS && c->train_phase != ONTC_TRAIN_ERROR)) {
     c->last_error = ONTC_INVALID_STATE;
     return;
   }
@@ -1219,8 +1245,10 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
   if (!e) e = cudaMemset(c->Wv.p, 0, c->nW * sizeof(float));
   if (!e) e = c->losses.alloc((size_t)std::max(c->batch_count, 1));
   if (!e) e = cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double));
-  if (e) c->last_error = ONTC_CUDA_FAILURE;
-  c->train_phase = ONTC_TRAIN_IN_PROGRESS;
+  // a failed start (no step-loss buffer, a failed upload) leaves the context in TrainError: no
+  // step may run on it until ontc_begin_training succeeds
+  if (e) c->last_error = e == cudaErrorMemoryAllocation ? ONTC_ALLOCATION_FAILURE : ONTC_CUDA_FAILURE;
+  c->train_phase = e ? ONTC_TRAIN_ERROR : ONTC_TRAIN_IN_PROGRESS;
 }
 
 int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
@@ -1228,37 +1256,45 @@ int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
   if (!c->initialized || !o) return ONTC_INVALID_STATE;
   if (o->precision != ONTC_PRECISION_FP32 && o->precision != ONTC_PRECISION_BF16) return ONTC_INVALID_STATE;
   if (c->batch_i > 0) return ONTC_INVALID_STATE;
+  if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
+  if (o->latent_adam != ONTC_LATENT_ADAM_DEFERRED && o->latent_adam != ONTC_LATENT_ADAM_DENSE) return ONTC_INVALID_STATE;
+  if (o->calibration != ONTC_CALIBRATION_UPSTREAM && o->calibration != ONTC_CALIBRATION_SEARCH) return ONTC_INVALID_STATE;
+  if (o->noise_mode == ONTC_NOISE_UPSTREAM && !c->manifest_loaded) return ONTC_INVALID_STATE;
+  // a buffer the options need that cannot be had leaves the context in TrainError (no step may
+  // run with a missing step-loss or noise buffer) until ontc_begin_training succeeds again
+  auto fail = [&](int r) {
+    c->last_error = r;
+    if (c->manifest_loaded) c->train_phase = ONTC_TRAIN_ERROR;
+    return r;
+  };
   c->precision = o->precision;
   if (o->steps_override > 0) {
     c->batch_count = o->steps_override;
     c->lock_i = (95 * c->batch_count) / 100;
     if (c->manifest_loaded) {
-      if (c->losses.alloc((size_t)c->batch_count) || cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double)))
-        return ONTC_ALLOCATION_FAILURE;
+      if (c->losses.alloc((size_t)c->batch_count)) return fail(ONTC_ALLOCATION_FAILURE);
+      if (cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double))) return fail(ONTC_CUDA_FAILURE);
     }
   }
   if (o->has_lock_step) c->lock_i = std::max(0, o->lock_step);
-  if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
-  if (o->latent_adam != ONTC_LATENT_ADAM_DEFERRED && o->latent_adam != ONTC_LATENT_ADAM_DENSE) return ONTC_INVALID_STATE;
-  if (o->calibration != ONTC_CALIBRATION_UPSTREAM && o->calibration != ONTC_CALIBRATION_SEARCH) return ONTC_INVALID_STATE;
   c->calibration = o->calibration;
   // the deferred kernels are compiled per profile channel pair; anything else runs dense
   c->optimizer = deferred_supported(c->C0, c->C1) ? o->latent_adam : ONTC_LATENT_ADAM_DENSE;
-  c->noise_mode = o->noise_mode;
-  if (c->noise_mode == ONTC_NOISE_UPSTREAM) {
-    if (!c->manifest_loaded) return ONTC_INVALID_STATE;
+  if (o->noise_mode == ONTC_NOISE_UPSTREAM) {
     if (!c->noise_states.p) {
-      if (c->noise_states.alloc(noise_state_bytes(ontc_context::kNoiseStates))) return ONTC_ALLOCATION_FAILURE;
-      if (launch_noise_init(c->noise_states.p, ontc_context::kNoiseStates, c->stream)) return ONTC_CUDA_FAILURE;
+      if (c->noise_states.alloc(noise_state_bytes(ontc_context::kNoiseStates))) return fail(ONTC_ALLOCATION_FAILURE);
+      if (launch_noise_init(c->noise_states.p, ontc_context::kNoiseStates, c->stream)) return fail(ONTC_CUDA_FAILURE);
       c->launches++;
     }
     for (int g = 0; g < 2; g++) {
       if (!c->noise_buf[g].p) {
-        if (c->noise_buf[g].alloc(c->level_elems(g, 0))) return ONTC_ALLOCATION_FAILURE;
-        if (cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream)) return ONTC_CUDA_FAILURE;
+        if (c->noise_buf[g].alloc(c->level_elems(g, 0))) return fail(ONTC_ALLOCATION_FAILURE);
+        if (cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream))
+          return fail(ONTC_CUDA_FAILURE);
       }
     }
   }
+  c->noise_mode = o->noise_mode;  // set once its buffers exist
   return ONTC_SUCCESS;
 }
 
@@ -1383,8 +1419,12 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
           make_foot(c, s, c->h_foots[k], c->foot_in[k]);
         }
       }
+      s.exact_grad = c->exact_grad ? 1 : 0;
       s.lr_grid = cosine_annealing(0.0f, 0.01f, c->batch_count, bi);
-      s.lr_dec = cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
+      // the exact-gradient test mode holds the decoder fixed: the two tile groups of a CTA add
+      // their weight-gradient products to shared TMEM accumulators in arrival order, so the
+      // decoder gradient is not bit-reproducible from run to run
+      s.lr_dec = c->exact_grad ? 0.0f : cosine_annealing(0.0f, 0.005f, c->batch_count, bi);
       s.step = bi;
     }
     drawn = std::max(drawn, std::min(cnt, k1 + 1));
@@ -1972,6 +2012,44 @@ int ontc_debug_package(ontc_context* c, int32_t mip, uint8_t* out)
   if (!c->manifest_loaded || mip < 0 || mip >= c->mips) return ONTC_INVALID_STATE;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!e) e = cudaMemcpy(out, c->package[mip].p, c->package[mip].n, cudaMemcpyDeviceToHost);
+  return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
+}
+
+int64_t ontc_debug_fail_device_alloc(int64_t n)
+{
+  const int64_t done = g_dev_allocs.load();
+  g_fail_alloc.store(n > 0 ? done + n : 0);
+  return done;
+}
+
+int ontc_debug_exact_gradients(ontc_context* c, int32_t enable)
+{
+  if (!c) return ONTC_INVALID_STATE;
+  c->exact_grad = enable != 0;
+  return ONTC_SUCCESS;
+}
+
+int ontc_debug_complete(ontc_context* c, const float* s_a)
+{
+  if (!c || !c->manifest_loaded ||
+      (c->train_phase != ONTC_TRAIN_IN_PROGRESS && c->train_phase != ONTC_TRAIN_COMPLETE))
+    return ONTC_INVALID_STATE;
+  cudaError_t e = drain_side(c);
+  if (!e) e = flush_latents(c);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (e) return ONTC_CUDA_FAILURE;
+  c->batch_i = c->batch_count;
+  c->train_phase = ONTC_TRAIN_COMPLETE;
+  e = complete_training(c);
+  if (!e && s_a) {
+    std::vector<float> Wh(c->nW);
+    e = cudaMemcpy(Wh.data(), c->W.p, c->nW * sizeof(float), cudaMemcpyDeviceToHost);
+    if (!e) {
+      c->caldata.s_a1 = s_a[0];
+      c->caldata.s_a2 = s_a[1];
+      build_blob(c, Wh, s_a[0], s_a[1], false, c->decoder_host.data());
+    }
+  }
   return e ? ONTC_CUDA_FAILURE : ONTC_SUCCESS;
 }
 

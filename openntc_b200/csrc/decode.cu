@@ -513,6 +513,11 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
           lod = A.lod[i];
         }
         features<SH>(A, u, v, lod, w, tables_s);
+        if (A.feat_out) {
+          uint4* fo = reinterpret_cast<uint4*>(A.feat_out + i * 24);
+#pragma unroll
+          for (int j = 0; j < Kp / 16; j++) fo[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+        }
       } else {
 #pragma unroll
         for (int j = 0; j < Kp / 4; j++) w[j] = 0u;

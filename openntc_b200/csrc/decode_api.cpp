@@ -12,6 +12,7 @@
 
 #include "kernels.h"
 #include "ontc.h"
+#include "ontc_debug.h"
 
 struct ontc_decoder {
   int profile = 0;
@@ -336,6 +337,27 @@ void ontc_decoder_destroy(ontc_decoder* d)
   cudaStreamSynchronize(d->stream);
   release(d);
   delete d;
+}
+
+int ontc_debug_decode_features(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n, int8_t* d_out)
+{
+  if (!d || d->mode != ONTC_DECODE_INT8 || n < 0 || (n > 0 && (!d_uv || !d_lod || !d_out))) return ONTC_INVALID_STATE;
+  if (n == 0) return ONTC_SUCCESS;
+  float* outs = nullptr;  // the decoded channels, discarded
+  if (cudaMalloc(&outs, (size_t)n * d->k.channel_count * sizeof(float)) != cudaSuccess) return ONTC_ALLOCATION_FAILURE;
+  cudaError_t e = cudaMemsetAsync(d_out, 0, (size_t)n * 96, d->stream);
+  if (!e) {
+    ontc::DecodeArgs a = base_args(d);
+    a.uv = d_uv;
+    a.lod = d_lod;
+    a.n = n;
+    a.out = outs;
+    a.feat_out = reinterpret_cast<uint32_t*>(d_out);
+    e = ontc::launch_decode(d->profile, a, d->stream);
+  }
+  if (!e) e = cudaStreamSynchronize(d->stream);
+  cudaFree(outs);
+  return e == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
 }
 
 int ontc_decode(ontc_decoder* d, const float* d_uv, const int32_t* d_lod, int64_t n, float* d_out)

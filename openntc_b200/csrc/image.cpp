@@ -1,6 +1,7 @@
 // PNM and PNG decoding to RGBA8 (see image.h).  PNG per RFC 2083 with zlib inflate.
 #include "image.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -79,6 +80,51 @@ int paeth(int a, int b, int c)
   return c;
 }
 
+// Bytes of one filtered row of a (sub-)image w pixels wide at `bits` bits per pixel.
+size_t row_bytes(size_t w, int bits) { return (w * (size_t)bits + 7) / 8; }
+
+// Reverses the per-row filters (RFC 2083 section 6) of one h-row sub-image in place in `rows`
+// (each row: a filter byte then rb bytes), writing the unfiltered rows to out[h][rb].
+bool unfilter(const uint8_t* rows, size_t rb, size_t h, size_t bpp, std::vector<uint8_t>& out)
+{
+  out.assign(rb * h, 0);
+  for (size_t y = 0; y < h; y++) {
+    const uint8_t* src = rows + (rb + 1) * y + 1;
+    const int filter = rows[(rb + 1) * y];
+    uint8_t* cur = &out[rb * y];
+    const uint8_t* prev = y > 0 ? &out[rb * (y - 1)] : nullptr;
+    for (size_t i = 0; i < rb; i++) {
+      const int a = i >= bpp ? cur[i - bpp] : 0;
+      const int b = prev ? prev[i] : 0;
+      const int c = (prev && i >= bpp) ? prev[i - bpp] : 0;
+      int v = src[i];
+      switch (filter) {
+        case 0: break;
+        case 1: v += a; break;
+        case 2: v += b; break;
+        case 3: v += (a + b) >> 1; break;
+        case 4: v += paeth(a, b, c); break;
+        default: return false;
+      }
+      cur[i] = (uint8_t)v;
+    }
+  }
+  return true;
+}
+
+// Sample `comp` of pixel x of an unfiltered row at bit depth `depth` (1, 2, 4, 8 or 16).
+int row_sample(const uint8_t* row, size_t x, int comps, int comp, int depth)
+{
+  if (depth == 16) return (row[(x * comps + comp) * 2] << 8) | row[(x * comps + comp) * 2 + 1];
+  if (depth == 8) return row[x * comps + comp];
+  const size_t bit = (x * comps + comp) * (size_t)depth;  // sub-byte samples: one component
+  return (row[bit >> 3] >> (8 - depth - (int)(bit & 7))) & ((1 << depth) - 1);
+}
+
+// PNG to RGBA8 with stb_image's expansion (what upstream's stbi_load(..., 4) returns,
+// libopenntc.cpp:1302): grey g -> (g, g, g, 255), grey+alpha -> (g, g, g, a), palette via
+// PLTE/tRNS, 16-bit samples keep their high byte, 1/2/4-bit grey scaled to 8 bits (x 255 / 85 /
+// 17), tRNS colour keys give alpha 0.  Non-interlaced and Adam7-interlaced images.
 bool decode_png(const std::vector<uint8_t>& d, std::vector<uint8_t>& rgba, int& w, int& h)
 {
   static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
@@ -110,71 +156,81 @@ bool decode_png(const std::vector<uint8_t>& d, std::vector<uint8_t>& rgba, int& 
     }
     p += 12 + (size_t)len;
   }
-  if (!have_ihdr || interlace != 0 || (depth != 8 && depth != 16) || w <= 0 || h <= 0) return false;
+  if (!have_ihdr || interlace > 1 || w <= 0 || h <= 0 || w > (1 << 24) || h > (1 << 24)) return false;
   int comps;
+  bool depth_ok;
   switch (ctype) {
-    case 0: comps = 1; break;
-    case 2: comps = 3; break;
-    case 3: comps = 1; if (depth != 8 || plte.empty()) return false; break;
-    case 4: comps = 2; break;
-    case 6: comps = 4; break;
+    case 0: comps = 1; depth_ok = depth == 1 || depth == 2 || depth == 4 || depth == 8 || depth == 16; break;
+    case 2: comps = 3; depth_ok = depth == 8 || depth == 16; break;
+    case 3: comps = 1; depth_ok = (depth == 1 || depth == 2 || depth == 4 || depth == 8) && !plte.empty(); break;
+    case 4: comps = 2; depth_ok = depth == 8 || depth == 16; break;
+    case 6: comps = 4; depth_ok = depth == 8 || depth == 16; break;
     default: return false;
   }
-  const size_t bpp = (size_t)comps * (depth / 8);
-  const size_t stride = (size_t)w * bpp;
-  std::vector<uint8_t> raw((stride + 1) * h);
+  if (!depth_ok) return false;
+  const int bits = comps * depth;
+  const size_t bpp = std::max<size_t>(1, (size_t)bits / 8);  // filter distance in bytes
+  // passes: x0, y0, dx, dy (Adam7, or one pass over the whole image)
+  static const int adam7[7][4] = {{0, 0, 8, 8}, {4, 0, 8, 8}, {0, 4, 4, 8}, {2, 0, 4, 4},
+                                  {0, 2, 2, 4}, {1, 0, 2, 2}, {0, 1, 1, 2}};
+  static const int whole[1][4] = {{0, 0, 1, 1}};
+  const int (*passes)[4] = interlace ? adam7 : whole;
+  const int npass = interlace ? 7 : 1;
+  size_t pw[7], ph[7], total = 0;
+  for (int k = 0; k < npass; k++) {
+    const int x0 = passes[k][0], y0 = passes[k][1], dx = passes[k][2], dy = passes[k][3];
+    pw[k] = (size_t)w > (size_t)x0 ? ((size_t)w - x0 + dx - 1) / dx : 0;
+    ph[k] = (size_t)h > (size_t)y0 ? ((size_t)h - y0 + dy - 1) / dy : 0;
+    if (pw[k] && ph[k]) total += ph[k] * (row_bytes(pw[k], bits) + 1);
+  }
+  std::vector<uint8_t> raw(total);
   uLongf out_len = (uLongf)raw.size();
   if (uncompress(raw.data(), &out_len, idat.data(), (uLong)idat.size()) != Z_OK || out_len != raw.size()) return false;
-  std::vector<uint8_t> img(stride * h);
-  for (int y = 0; y < h; y++) {
-    const uint8_t* src = &raw[(stride + 1) * y + 1];
-    const int filter = raw[(stride + 1) * y];
-    uint8_t* cur = &img[stride * y];
-    const uint8_t* prev = y > 0 ? &img[stride * (y - 1)] : nullptr;
-    for (size_t i = 0; i < stride; i++) {
-      const int a = i >= bpp ? cur[i - bpp] : 0;
-      const int b = prev ? prev[i] : 0;
-      const int c = (prev && i >= bpp) ? prev[i - bpp] : 0;
-      int v = src[i];
-      switch (filter) {
-        case 0: break;
-        case 1: v += a; break;
-        case 2: v += b; break;
-        case 3: v += (a + b) >> 1; break;
-        case 4: v += paeth(a, b, c); break;
-        default: return false;
+  // raw samples per pixel, unscaled (up to 16 bits)
+  const size_t n = (size_t)w * h;
+  std::vector<uint16_t> px(n * comps);
+  size_t off = 0;
+  std::vector<uint8_t> rows;
+  for (int k = 0; k < npass; k++) {
+    if (!pw[k] || !ph[k]) continue;
+    const size_t rb = row_bytes(pw[k], bits);
+    if (!unfilter(&raw[off], rb, ph[k], bpp, rows)) return false;
+    off += ph[k] * (rb + 1);
+    for (size_t yy = 0; yy < ph[k]; yy++) {
+      const size_t y = passes[k][1] + yy * passes[k][3];
+      for (size_t xx = 0; xx < pw[k]; xx++) {
+        const size_t x = passes[k][0] + xx * passes[k][2];
+        for (int c = 0; c < comps; c++)
+          px[(y * w + x) * comps + c] = (uint16_t)row_sample(&rows[rb * yy], xx, comps, c, depth);
       }
-      cur[i] = (uint8_t)v;
     }
   }
-  const size_t n = (size_t)w * h;
-  rgba.resize(n * 4);
-  const int sb = depth / 8;  // 16-bit samples keep their high byte
-  auto sample = [&](size_t px, int comp) -> int { return img[px * bpp + (size_t)comp * sb]; };
-  auto sample16 = [&](size_t px, int comp) -> int {
-    return sb == 2 ? (img[px * bpp + comp * 2] << 8) | img[px * bpp + comp * 2 + 1] : img[px * bpp + comp];
+  // 8-bit value of a sample: the high byte of 16-bit samples, grey scaled up from 1/2/4 bits
+  const int scale = depth == 1 ? 255 : depth == 2 ? 85 : depth == 4 ? 17 : 1;
+  auto to8 = [&](int v) -> uint8_t { return (uint8_t)(depth == 16 ? v >> 8 : v * scale); };
+  // whether sample v of component c equals the tRNS colour key: 16-bit samples against the whole
+  // key, others (as stb_image compares them) in the 8-bit domain against the key's low byte scaled
+  auto keyed = [&](int c, int v) -> bool {
+    const int k = (trns[2 * c] << 8) | trns[2 * c + 1];
+    return depth == 16 ? v == k : to8(v) == (uint8_t)((k & 255) * scale);
   };
+  rgba.resize(n * 4);
   for (size_t i = 0; i < n; i++) {
+    const uint16_t* s = &px[i * comps];
     uint8_t* o = &rgba[i * 4];
     switch (ctype) {
-      case 0: {
-        o[0] = o[1] = o[2] = (uint8_t)sample(i, 0);
-        o[3] = 255;
-        if (trns.size() >= 2 && sample16(i, 0) == (int)((trns[0] << 8) | trns[1])) o[3] = 0;
+      case 0:
+        o[0] = o[1] = o[2] = to8(s[0]);
+        o[3] = (trns.size() >= 2 && keyed(0, s[0])) ? 0 : 255;
         break;
-      }
-      case 2: {
-        o[0] = (uint8_t)sample(i, 0);
-        o[1] = (uint8_t)sample(i, 1);
-        o[2] = (uint8_t)sample(i, 2);
-        o[3] = 255;
-        if (trns.size() >= 6 && sample16(i, 0) == (int)((trns[0] << 8) | trns[1]) &&
-            sample16(i, 1) == (int)((trns[2] << 8) | trns[3]) && sample16(i, 2) == (int)((trns[4] << 8) | trns[5]))
-          o[3] = 0;
+      case 2:
+        o[0] = to8(s[0]);
+        o[1] = to8(s[1]);
+        o[2] = to8(s[2]);
+        o[3] = (trns.size() >= 6 && keyed(0, s[0]) && keyed(1, s[1]) && keyed(2, s[2])) ? 0 : 255;
         break;
-      }
       case 3: {
-        const int idx = img[i];
+        const int idx = s[0];
         if ((size_t)idx * 3 + 2 >= plte.size()) return false;
         o[0] = plte[idx * 3];
         o[1] = plte[idx * 3 + 1];
@@ -182,17 +238,15 @@ bool decode_png(const std::vector<uint8_t>& d, std::vector<uint8_t>& rgba, int& 
         o[3] = (size_t)idx < trns.size() ? trns[idx] : 255;
         break;
       }
-      case 4: {
-        o[0] = o[1] = o[2] = (uint8_t)sample(i, 0);
-        o[3] = (uint8_t)sample(i, 1);
+      case 4:
+        o[0] = o[1] = o[2] = to8(s[0]);
+        o[3] = to8(s[1]);
         break;
-      }
-      default: {
-        o[0] = (uint8_t)sample(i, 0);
-        o[1] = (uint8_t)sample(i, 1);
-        o[2] = (uint8_t)sample(i, 2);
-        o[3] = (uint8_t)sample(i, 3);
-      }
+      default:
+        o[0] = to8(s[0]);
+        o[1] = to8(s[1]);
+        o[2] = to8(s[2]);
+        o[3] = to8(s[3]);
     }
   }
   return true;
@@ -209,3 +263,17 @@ bool load_image_rgba8(const std::string& path, std::vector<uint8_t>& rgba, int& 
 }
 
 }  // namespace ontc
+
+#include "ontc_debug.h"
+
+extern "C" int ontc_debug_load_image(const char* path, int32_t* width, int32_t* height, uint8_t* rgba)
+{
+  if (!path || !width || !height) return ONTC_INVALID_STATE;
+  std::vector<uint8_t> px;
+  int w = 0, h = 0;
+  if (!ontc::load_image_rgba8(path, px, w, h)) return ONTC_FILE_NOT_FOUND;
+  *width = w;
+  *height = h;
+  if (rgba) memcpy(rgba, px.data(), px.size());
+  return ONTC_SUCCESS;
+}

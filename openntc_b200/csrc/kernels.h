@@ -36,6 +36,9 @@ struct DecodeArgs {
   bool material = false;
   int8_t material_dst[16] = {};
   uint32_t material_present = 0;
+  // test hook (ontc_debug_decode_features): each sample's Kp feature bytes also go to
+  // feat_out[i * 24 ..] (rows of 96 bytes)
+  uint32_t* feat_out = nullptr;
 };
 cudaError_t launch_decode(int profile, const DecodeArgs& args, cudaStream_t stream);
 // The float-model decoders (decode_float.cu): the trained fp32 decoder weights evaluated on the

@@ -56,6 +56,9 @@ extern "C" int ontc_lanczos_down_noalloc(const uint8_t* d_src, int32_t dim, int3
     return ONTC_INVALID_DIMENSION;
   float* tmp = nullptr;
   if (scratch_address(&tmp) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  // clear a launch error left by earlier, unrelated work, so the status below is this call's
+  // (a sticky error from a faulted context cannot be cleared and is still reported)
+  (void)cudaGetLastError();
   cudaError_t e = ontc::launch_lanczos_down(d_src, dim, ch, tmp, d_dst, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? ONTC_SUCCESS : ONTC_CUDA_FAILURE;
 }

@@ -264,6 +264,18 @@ __device__ __forceinline__ void build_masks(const StepRec& s, int d0, int d1, co
   }
 }
 
+// Test mode (StepRec::exact_grad): a feature gradient replaced by n * 2^-24 with
+// n = clamp(rint(v * 2^24), -15, 15).  Every latent-gradient term is then such a value times a
+// bilinear weight with at most 8 fractional bits (the mip-to-g1 cell ratio is at most 8 in
+// every profile), so each latent's gradient is a multiple of 2^-32 below 2^-12 in magnitude
+// (at most 256 texels reach a g1 cell): every partial sum is exact, and the float atomics give
+// the same bits in any order.  Lets a test compare two optimiser schedules bit for bit.
+__device__ __forceinline__ float exact_dyadic(float v)
+{
+  const float n = fminf(fmaxf(rintf(v * 16777216.0f), -15.0f), 15.0f);
+  return n * (1.0f / 16777216.0f);
+}
+
 // v / d for the small operands of the box loops (v < 2^20, d >= 1) with one multiply: with
 // inv = RN(1/d), (v + 0.5) * inv stays within 2^-3 / d of v / d + 0.5 / d, strictly between the
 // two integers around it, so its floor is the quotient (replaces a 32-bit division per item).
@@ -840,6 +852,10 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 #pragma unroll
         for (int c = 0; c < KH; c += 8) ptx::ld8(lwin + half * KH + c, dx + c);
         ptx::ld_wait();
+        if (s.exact_grad) {
+#pragma unroll
+          for (int c = 0; c < KH; c++) dx[c] = exact_dyadic(dx[c]);
+        }
 #pragma unroll
         for (int c = 0; c < KH; c += 4)
           *reinterpret_cast<float4*>(dxs + row * LD + half * KH + c) = make_float4(dx[c], dx[c + 1], dx[c + 2], dx[c + 3]);

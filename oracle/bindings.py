@@ -318,6 +318,14 @@ class RefContext:
         p = self.L.ref_mip_host(self.h, source, mip)
         return np.ctypeslib.as_array(p, shape=(size,)).copy()
 
+    def compressed(self):
+        """Upstream's GetCompressedData() (libopenntc.cpp:1055-1101) as the layout-identical
+        ontc_compressed_data mirror; its pointers borrow upstream's host buffers."""
+        from openntc_b200 import _abi
+        cd = _abi.CompressedData()
+        self.L.ref_get_compressed(self.h, C.byref(cd))
+        return cd
+
     def decoder(self) -> np.ndarray:
         n = C.c_longlong()
         p = self.L.ref_decoder_host(self.h, C.byref(n))

@@ -33,6 +33,8 @@ def _noalloc(lib, torch, img, stream):
     dim, ch = img.shape[0], img.shape[2]
     src = torch.from_numpy(img).cuda()
     dst = torch.full((dim // 2, dim // 2, ch), 7, dtype=torch.uint8, device="cuda")
+    # src and dst were written on torch's current stream: the reduction's stream waits for them
+    stream.wait_stream(torch.cuda.current_stream())
     r = lib.ontc_lanczos_down_noalloc(C.c_void_p(src.data_ptr()), dim, ch, C.c_void_p(dst.data_ptr()),
                                       C.c_void_p(stream.cuda_stream))
     assert r == 0, r
@@ -80,3 +82,28 @@ def test_noalloc_rejects_images_beyond_its_scratch(lib, torch_cuda):
     assert lib.ontc_lanczos_down_noalloc(None, 64, 1, C.c_void_p(dst.data_ptr()), None) == 1
     torch.cuda.synchronize()
     assert not dst.any()
+
+
+def test_noalloc_calls_allocate_no_device_memory(lib, torch_cuda):
+    """The property the entry point exists for: after a first call (which looks the scratch array
+    up), further calls leave the device's free memory unchanged."""
+    torch = torch_cuda
+    img = _image(512, 4, 11)
+    src = torch.from_numpy(img).cuda()
+    dst = torch.zeros((256, 256, 4), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+
+    def call():
+        assert lib.ontc_lanczos_down_noalloc(C.c_void_p(src.data_ptr()), 512, 4, C.c_void_p(dst.data_ptr()),
+                                             C.c_void_p(stream.cuda_stream)) == 0
+        stream.synchronize()
+
+    call()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(8):
+        call()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert np.array_equal(dst.cpu().numpy(), _allocating(lib, img))
