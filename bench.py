@@ -208,7 +208,7 @@ def run_ours(args):
             barrier()
             assert p.result == 0, p
             region_ms.append(max_over_ranks(ev0.elapsed_time(ev1)))
-            if sum(region_ms) >= MIN_TIMED_MS or len(region_ms) >= reps_cap:
+            if sum(region_ms) >= args.min_timed_ms or len(region_ms) >= reps_cap:
                 break
     reps = len(region_ms)
     launches = (ctx.kernel_launches() - l0) / reps
@@ -232,7 +232,7 @@ def run_ours(args):
         barrier()
         assert p.result == 0 and all(l > 0 for l in losses)
         e2e_region.append(max_over_ranks(t1 - t0))
-        if sum(e2e_region) >= MIN_TIMED_MS / 1e3 or len(e2e_region) >= e2e_reps_cap:
+        if sum(e2e_region) >= args.min_timed_ms / 1e3 or len(e2e_region) >= e2e_reps_cap:
             break
     e2e_s = statistics.median(e2e_region)
 
@@ -470,7 +470,7 @@ def run_decode(args, embedded=False):
             ev1.record(stream)
             torch.cuda.synchronize()
             region_ms.append(ev0.elapsed_time(ev1))
-            if sum(region_ms) >= MIN_TIMED_MS or len(region_ms) >= 200:
+            if sum(region_ms) >= args.min_timed_ms or len(region_ms) >= 200:
                 break
     assert dec.status() == 0
     ms = statistics.median(region_ms) / K
@@ -683,7 +683,7 @@ def run_reference(args):
             ms_k, prog, err = ref.time_train(K)
             assert err == 0 and prog[1] == 0, (err, prog)
             region_ms.append(ms_k)
-            if sum(region_ms) >= MIN_TIMED_MS or len(region_ms) >= reps_cap:
+            if sum(region_ms) >= args.min_timed_ms or len(region_ms) >= reps_cap:
                 break
     ms = statistics.median(region_ms)
     B = WORKLOAD["batch_texels"]
@@ -694,7 +694,7 @@ def run_reference(args):
         t0 = time.perf_counter()
         ref.train(K)
         e2e_region.append(time.perf_counter() - t0)
-        if sum(e2e_region) >= MIN_TIMED_MS / 1e3 or len(e2e_region) >= e2e_cap:
+        if sum(e2e_region) >= args.min_timed_ms / 1e3 or len(e2e_region) >= e2e_cap:
             break
     e2e_s = statistics.median(e2e_region)
     ref.close()
@@ -760,6 +760,8 @@ def main():
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
     ap.add_argument("--latent-adam", choices=["deferred", "dense"], default="deferred")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-timed-ms", type=float, default=MIN_TIMED_MS,
+                    help="repeat each K-step timed region until this much time (0: one region, for profiling)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload only: skip the s-to-PSNR run and the decode measurement")
     ap.add_argument("--workload", choices=["train", "decode", "batch"], default="train")
