@@ -230,6 +230,18 @@ ONTC_HD void gather_geometry(int x, int y, int mip_dim, int g0_dim, int g1_dim, 
   }
 }
 
+// The corner cells (lower and upper, clamped into the grid) that texels a..b of a mip of size
+// `mip` reach in a grid of size gd, along one axis: gather_geometry's arithmetic.  First cell
+// lo, count n.
+ONTC_HD void foot_span(int a, int b, int mip, int gd, int& lo, int& n)
+{
+  const float rm = rcp_pow2(mip);
+  const float ua = ((float)a + 0.5f) * rm, ub = ((float)b + 0.5f) * rm;
+  const int l = (int)floorf(ua * (float)gd - 0.5f), h = (int)floorf(ub * (float)gd - 0.5f) + 1;
+  lo = clampi(l, 0, gd - 1);
+  n = clampi(h, 0, gd - 1) - lo + 1;
+}
+
 // Triangle-wave positional encoding, periods 8/4/2 x (x, y) x phase (0, P/4)
 // (ntc_kernel.cu:145-165).  All intermediate values are exact in fp32.
 ONTC_HD float pos_enc(int x, int y, int idx)

@@ -237,6 +237,7 @@ struct ontc_context {
   bool side_pending = false;
   DBuf<uint8_t> package[ONTC_MAX_MIPS];
   DBuf<uint32_t> packbuf;
+  LatentBoxes boxes[ONTC_MAX_MIPS] = {};  // the tile kernel's TMA staging per lod
   DBuf<int> tc_error;
   DBuf<uint8_t> noise_states;   // upstream-mode cuRAND states (initialised once per context)
   DBuf<float> noise_buf[2];     // upstream-mode level noise buffers, level-0 sized
@@ -1119,6 +1120,17 @@ int ontc_load_manifest(ontc_context* c, const char* path)
   if (c->hist.alloc((size_t)c->levels * kHistRing)) return fail(ONTC_ALLOCATION_FAILURE);
   if (c->packbuf.alloc(std::max(c->level_elems(0, 0) * c->b0 / 32, c->level_elems(1, 0) * c->b1 / 32) + 4))
     return fail(ONTC_ALLOCATION_FAILURE);
+  // TMA staging boxes of each lod's level (no staging where the driver cannot encode tensor maps)
+  for (int m = 0; m < c->mips; m++) {
+    const int l = c->feature_level_for_lod(m);
+    const cudaError_t be = make_latent_boxes(c->lat[0][0][l].p, c->lat[1][0][l].p, c->g0_dim[l], c->g1_dim[l], c->C0,
+                                             c->C1, c->mip_dim[m], tc_box_capacity(), c->boxes[m]);
+    if (be == cudaErrorNotSupported) {
+      for (int j = 0; j < c->mips; j++) c->boxes[j].w0 = 0;
+      break;
+    }
+    if (be != cudaSuccess) return fail(ONTC_CUDA_FAILURE);
+  }
   c->g0_host_packed.assign(words0, 0);
   c->g1_host_packed.assign(words1, 0);
   size_t o0 = 0, o1 = 0;
@@ -1504,7 +1516,7 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       } else if (c->precision == ONTC_PRECISION_BF16) {
         grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
         cls = ONTC_KCLASS_UNITS_BF16;
-        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->stream);
+        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->boxes[s.lod], c->stream);
         if (e == cudaErrorNotSupported) {
           cudaGetLastError();
           grid = std::min(units, c->sms);
@@ -1950,7 +1962,7 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
   if (!e) {
     if (c->precision == ONTC_PRECISION_BF16) {
       grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
-      e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->stream);
+      e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->boxes[s.lod], c->stream);
       if (e == cudaErrorNotSupported) {
         cudaGetLastError();
         grid = std::min(units, c->sms);

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -95,13 +96,30 @@ struct TileOut {
   float* calib_max;      // [2] running max |a0|, |a1| as ordered ints (kCalib)
 };
 
+// TMA staging of a 16 x 8 texel unit's latent boxes at one lod (tile kernel): tensor maps of
+// the lod's level and the fixed box sizes that cover every unit footprint at that lod.
+struct LatentBoxes {
+  CUtensorMap g0;          // 3-D {C0, d0, d0} view of the level's g0 latents, box {C0, w0, h0}
+  CUtensorMap g1;          // 2-D {d1 * C1, d1} view of g1, box {w1 * C1, h1}
+  int32_t w0, h0, w1, h1;  // box sizes in cells; w0 == 0: units at this lod are not staged
+  int32_t g1_shift;        // 1: the g1 box starts at the even cell at or below the footprint's first
+  uint32_t bytes;          // bytes the two loads deliver
+  uint32_t g1_off;         // float offset of the g1 box in a staging buffer (128-byte aligned)
+};
+// Builds the boxes of lod `lod` for latents p0 / p1 of grid sizes d0 / d1 (staging buffer of
+// `cap_floats`); w0 = 0 when the footprint does not fit.  cudaSuccess or the driver's error.
+cudaError_t make_latent_boxes(const float* p0, const float* p1, int d0, int d1, int C0, int C1, int mip_dim,
+                              int cap_floats, LatentBoxes& out);
+
 // ---- training / eval units
 size_t simt_smem_bytes(int F);
 cudaError_t launch_simt_units(int mode, const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
                               cudaStream_t stream);
 // BF16 tcgen05 path; returns cudaErrorNotSupported when the profile has no tcgen05 variant
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
-                            int* d_error, cudaStream_t stream);
+                            int* d_error, const LatentBoxes& boxes, cudaStream_t stream);
+// the staging buffer the tile kernel gives a unit's latent boxes, in floats
+int tc_box_capacity();
 int tc_max_grid();
 
 // ---- optimiser: decoder Adam (reducing `grid` partials) + dense latent Adam/clamp/zero

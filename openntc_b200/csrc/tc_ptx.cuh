@@ -53,6 +53,32 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
   return false;
 }
 
+// Arrival of this thread on `bar` that also expects `bytes` of asynchronous (TMA) writes.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// TMA tile loads (no multicast) of a box of a global tensor into shared memory, completing
+// on `bar`.  The tensor map is a kernel parameter (__grid_constant__); coordinates are in
+// elements, innermost first.
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int c0, int c1, int c2, uint64_t* bar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_addr(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int c0, int c1, uint64_t* bar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // Asynchronous global -> shared copies (completion tracked per thread in commit groups).
 __device__ __forceinline__ void cp_async16(void* dst_smem, const void* src)
 {
@@ -113,6 +139,22 @@ __device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t 
 {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+// A shared-memory matrix descriptor kept as its two 32-bit halves: the descriptor of a tile a
+// further `byte_off` bytes on is one 32-bit add on the low half (the 14-bit start-address field
+// cannot carry into the next field: shared-memory addresses are below 256 KB).
+struct DescBase {
+  uint32_t lo, hi;
+  __device__ __forceinline__ uint64_t at(uint32_t byte_off) const
+  {
+    return ((uint64_t)hi << 32) | (uint64_t)(lo + (byte_off >> 4));
+  }
+};
+__device__ __forceinline__ DescBase desc_base(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+  const uint64_t d = desc(saddr, lbo, sbo);
+  return DescBase{(uint32_t)d, (uint32_t)(d >> 32)};
 }
 
 // Instruction descriptor, kind::f16 with bf16 A/B and fp32 D.

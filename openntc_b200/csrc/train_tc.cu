@@ -43,7 +43,7 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColW0 = 256;   // dW0     (<= 96 columns)
 constexpr uint32_t kColW1 = 352;   // dW1     (64)
 constexpr uint32_t kColWo = 416;   // dWout^T (16)
-constexpr int kFootFloats = 6144;  // per group, 24 KB: two staging buffers
+constexpr int kFootFloats = 7168;  // per group, 28 KB: two staging buffers
 constexpr int kFootBuf = kFootFloats / 2;
 constexpr int kMaxBoxW = 64;       // latent box limits of the owner-computes scatter
 constexpr int kMaxBoxH = 32;
@@ -189,20 +189,13 @@ struct Foot {
   int x0, y0, w, h;
 };
 
-__device__ __forceinline__ void foot_span(int a, int b, int mip, int gd, int& lo, int& n)
-{
-  // corner cells of texels a..b: gather_geometry's arithmetic, clamped the same way
-  const float rm = rcp_pow2(mip);
-  const float ua = ((float)a + 0.5f) * rm, ub = ((float)b + 0.5f) * rm;
-  const int l = (int)floorf(ua * (float)gd - 0.5f), h = (int)floorf(ub * (float)gd - 0.5f) + 1;
-  lo = clampi(l, 0, gd - 1);
-  n = clampi(h, 0, gd - 1) - lo + 1;
-}
-
-// True when the unit is a 16x8 texel block that does not wrap and whose g0/g1 boxes fit.
+// True when the unit is a 16x8 texel block that does not wrap and whose g0/g1 footprints fit the
+// lod's staging boxes (the g1 box may start one cell before the footprint, see stage_issue).
 template <class SH>
-__device__ __forceinline__ bool unit_footprint(const LevelArgs& L, const StepRec& s, int unit, Foot& f0, Foot& f1)
+__device__ __forceinline__ bool unit_footprint(const LevelArgs& L, const StepRec& s, const LatentBoxes& B, int unit,
+                                               Foot& f0, Foot& f1)
 {
+  if (B.w0 == 0) return false;
   const int lt = log2_pow2(s.tile_dim);
   if (lt < 4) return false;
   const int b0 = unit * kTile, gi = b0 >> (2 * lt), r0 = b0 & ((1 << (2 * lt)) - 1);
@@ -216,8 +209,7 @@ __device__ __forceinline__ bool unit_footprint(const LevelArgs& L, const StepRec
   foot_span(ya, ya + 7, s.mip_dim, d0, f0.y0, f0.h);
   foot_span(xa, xa + 15, s.mip_dim, d1, f1.x0, f1.w);
   foot_span(ya, ya + 7, s.mip_dim, d1, f1.y0, f1.h);
-  return f0.w <= kMaxBoxW && f0.h <= kMaxBoxH && f1.w <= kMaxBoxW && f1.h <= kMaxBoxH &&
-         f0.w * f0.h * SH::C0 + f1.w * f1.h * SH::C1 <= kFootBuf;
+  return f0.w <= B.w0 && f0.h <= B.h0 && f1.w + (f1.x0 & B.g1_shift) <= B.w1 && f1.h <= B.h1;
 }
 
 // Which texel columns / rows of a unit touch each box column / row, per corner side: bit t
@@ -284,40 +276,25 @@ __device__ __forceinline__ int div_small(int v, float inv)
   return (int)(((float)v + 0.5f) * inv);
 }
 
-// Starts the asynchronous copy of a unit's latent boxes into a staging buffer.  Thread gt
-// copies elements gt, gt + 256, ...; add_noise then treats the same elements, so each thread
-// only needs its own copies complete.
+// Starts the TMA loads of a unit's latent boxes into a staging buffer (one thread): the g0 box
+// {C0, w0, h0} at the footprint's first cell, the g1 box {w1 * C1, h1} at its first cell or,
+// when a g1 cell is not a multiple of 16 bytes (C1 = 10), at the even cell at or below it (the
+// innermost TMA coordinate must be a multiple of 16 bytes); both complete on `bar`.
 template <class SH>
-__device__ __forceinline__ void stage_copy(const LevelArgs& L, const Foot& f0, const Foot& f1, float* foot, int gt)
+__device__ __forceinline__ void stage_issue(const LatentBoxes& B, const Foot& f0, const Foot& f1, float* foot,
+                                            uint64_t* bar)
 {
-  {
-    constexpr int C0 = SH::C0;
-    const int d0 = L.d0;
-    const int rowq = f0.w * (C0 / 4);
-    const float inv = 1.0f / (float)rowq;
-    const float* p0 = L.p0;
-    for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
-      const int r = div_small(v, inv), q = v - r * rowq;
-      ptx::cp_async16(foot + r * f0.w * C0 + q * 4, p0 + ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4);
-    }
-  }
-  {
-    constexpr int C1 = SH::C1;
-    const int d1 = L.d1;
-    const int rowh = f1.w * (C1 / 2);
-    const float inv = 1.0f / (float)rowh;
-    const float* p1 = L.p1;
-    float* foot1 = foot + f0.w * f0.h * SH::C0;
-    for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
-      const int r = div_small(v, inv), q = v - r * rowh;
-      ptx::cp_async8(foot1 + r * f1.w * C1 + q * 2, p1 + ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2);
-    }
-  }
+  ptx::fence_proxy_async();  // earlier generic-proxy reads of this buffer before the async writes
+  ptx::mbar_arrive_expect_tx(bar, B.bytes);
+  ptx::tma_load_3d(foot, &B.g0, 0, f0.x0, f0.y0, bar);
+  ptx::tma_load_2d(foot + B.g1_off, &B.g1, (f1.x0 - (f1.x0 & B.g1_shift)) * SH::C1, f1.y0, bar);
 }
 
-// Adds this step's quantisation noise to the staged latents this thread copied.
+// Adds this step's quantisation noise to the staged latents of the unit's footprint (rows of
+// the boxes are B.w0 / B.w1 cells apart).
 template <class SH>
-__device__ __forceinline__ void stage_noise(const LevelArgs& L, const Foot& f0, const Foot& f1, float* foot, int gt)
+__device__ __forceinline__ void stage_noise(const LevelArgs& L, const LatentBoxes& B, const Foot& f0, const Foot& f1,
+                                            float* foot, int gt)
 {
   {
     constexpr int C0 = SH::C0;
@@ -327,7 +304,7 @@ __device__ __forceinline__ void stage_noise(const LevelArgs& L, const Foot& f0, 
     for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
       const int r = div_small(v, inv), q = v - r * rowq;
       const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
-      float4* dst = reinterpret_cast<float4*>(foot + r * f0.w * C0 + q * 4);
+      float4* dst = reinterpret_cast<float4*>(foot + r * B.w0 * C0 + q * 4);
       float4 val = *dst;
       val.x += level_noise(L, 0u, (uint32_t)e);
       val.y += level_noise(L, 0u, (uint32_t)(e + 1));
@@ -341,11 +318,11 @@ __device__ __forceinline__ void stage_noise(const LevelArgs& L, const Foot& f0, 
     const int d1 = L.d1;
     const int rowh = f1.w * (C1 / 2);
     const float inv = 1.0f / (float)rowh;
-    float* foot1 = foot + f0.w * f0.h * SH::C0;
+    float* foot1 = foot + B.g1_off + (f1.x0 & B.g1_shift) * C1;
     for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
       const int r = div_small(v, inv), q = v - r * rowh;
       const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
-      float2* dst = reinterpret_cast<float2*>(foot1 + r * f1.w * C1 + q * 2);
+      float2* dst = reinterpret_cast<float2*>(foot1 + r * B.w1 * C1 + q * 2);
       float2 val = *dst;
       val.x += level_noise(L, 1u, (uint32_t)e);
       val.y += level_noise(L, 1u, (uint32_t)(e + 1));
@@ -409,8 +386,8 @@ __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int r
 }
 
 template <class SH>
-__device__ __forceinline__ void gather_half(const LevelArgs& L, int x, int y, bool valid, int row, int half,
-                                           bool staged, const Foot& f0, const Foot& f1, const float* foot,
+__device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxes& B, int x, int y, bool valid, int row,
+                                           int half, bool staged, const Foot& f0, const Foot& f1, const float* foot,
                                            uint8_t* sX)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
@@ -441,7 +418,7 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, int x, int y, bo
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
-      const float* src = foot + ((cy - f0.y0) * f0.w + (cx - f0.x0)) * C0;
+      const float* src = foot + ((cy - f0.y0) * B.w0 + (cx - f0.x0)) * C0;
 #pragma unroll
       for (int c = 0; c < C0; c += 4) {
         const float4 q = *reinterpret_cast<const float4*>(src + c);
@@ -456,11 +433,11 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, int x, int y, bo
   float acc[C1];
 #pragma unroll
   for (int c = 0; c < C1; c++) acc[c] = 0.0f;
-  const float* foot1 = foot + f0.w * f0.h * C0;
+  const float* foot1 = foot + B.g1_off + (f1.x0 & B.g1_shift) * C1;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     const int cy = G.c1[k] >> l1, cx = G.c1[k] & (d1 - 1);
-    const float* src = foot1 + ((cy - f1.y0) * f1.w + (cx - f1.x0)) * C1;
+    const float* src = foot1 + ((cy - f1.y0) * B.w1 + (cx - f1.x0)) * C1;
 #pragma unroll
     for (int c = 0; c < C1; c += 2) {
       const float2 q = *reinterpret_cast<const float2*>(src + c);
@@ -548,13 +525,15 @@ __device__ __forceinline__ void tmem_st_zero16(uint32_t taddr)
 
 template <class SH>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut out, int* __restrict__ err)
+tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut out, int* __restrict__ err,
+               const __grid_constant__ LatentBoxes boxes)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp, F = SH::F;
   constexpr uint32_t SX = SH::SX;
   constexpr int KH = Kp / 2;  // dX columns per half row (a multiple of 8)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t tma_bars[2][2];  // [group][staging buffer]: latent boxes landed
   __shared__ uint32_t tmem_base_s;
   __shared__ int fail_s;
   __shared__ double red[kThreads / 32];
@@ -590,6 +569,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (tid == 0) {
     ptx::mbar_init(&bars[0], 1);
     ptx::mbar_init(&bars[1], 1);
+    for (int i = 0; i < 4; i++) ptx::mbar_init(&tma_bars[i >> 1][i & 1], 1);
     ptx::fence_mbar_init();
     fail_s = 0;
   }
@@ -651,18 +631,32 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   const uint32_t aX = ptx::smem_addr(gp.X), aP0 = ptx::smem_addr(gp.P0), aP1 = ptx::smem_addr(gp.P1);
   const uint32_t adY = ptx::smem_addr(gp.dY);
   const uint32_t aW0 = ptx::smem_addr(sW0), aW1 = ptx::smem_addr(sW1), aWo = ptx::smem_addr(sWo);
+  // matrix descriptors of this group's operand tiles and the shared weight tiles, K-major (k)
+  // and MN-major (m) views; a tile further on is one add (DescBase::at)
+  const ptx::DescBase dXk = ptx::desc_base(aX, 128, SX), dXm = ptx::desc_base(aX, SX, 128);
+  const ptx::DescBase dP0k = ptx::desc_base(aP0, 128, S64), dP0m = ptx::desc_base(aP0, S64, 128);
+  const ptx::DescBase dP1k = ptx::desc_base(aP1, 128, S64), dP1m = ptx::desc_base(aP1, S64, 128);
+  const ptx::DescBase dYm = ptx::desc_base(adY, S16, 128);
+  const ptx::DescBase dW0k = ptx::desc_base(aW0, 128, SX), dW0m = ptx::desc_base(aW0, SX, 128);
+  const ptx::DescBase dW1k = ptx::desc_base(aW1, 128, S64), dW1m = ptx::desc_base(aW1, S64, 128);
+  const ptx::DescBase dWok = ptx::desc_base(aWo, 128, S64);
   const int hc = half * 32;  // this thread's first column of a 64-column tile
 
-  // latent boxes: unit k's were copied (asynchronously) while unit k-1 ran
+  // latent boxes: unit k's were loaded (TMA, asynchronously) while unit k-1 ran, into the
+  // staging buffer the previous unit did not use; tph holds each buffer's next wait parity and
+  // inflight which buffers have loads not yet waited for
   const int ustride = gridDim.x * 2;
   Foot nf0 = {}, nf1 = {};
   bool nstaged = false;
   int pb = 0;
+  uint32_t tph = 0, inflight = 0;
   {
     const int u0 = blockIdx.x * 2 + g;
-    nstaged = u0 < ntiles && unit_footprint<SH>(L, s, u0, nf0, nf1);
-    if (nstaged) stage_copy<SH>(L, nf0, nf1, gp.foot, gt);
-    ptx::cp_async_commit();
+    nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
+    if (nstaged) {
+      if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
+      inflight |= 1u;
+    }
   }
 
   for (int unit = blockIdx.x * 2 + g; unit < ntiles; unit += ustride) {
@@ -684,20 +678,29 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     }
     const Foot f0 = nf0, f1 = nf1;
     const bool staged = nstaged;
-    float* foot = gp.foot + pb * kFootBuf;
+    const int cur = pb;
+    float* foot = gp.foot + cur * kFootBuf;
     {
-      // start the next unit's copy into the other buffer (its last reader, the gather of
+      // start the next unit's loads into the other buffer (its last reader, the gather of
       // the unit before this one, finished several group barriers ago)
       const int nu = unit + ustride;
-      nstaged = nu < ntiles && unit_footprint<SH>(L, s, nu, nf0, nf1);
-      if (nstaged) stage_copy<SH>(L, nf0, nf1, gp.foot + (pb ^ 1) * kFootBuf, gt);
-      ptx::cp_async_commit();
+      nstaged = nu < ntiles && unit_footprint<SH>(L, s, boxes, nu, nf0, nf1);
+      if (nstaged) {
+        if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot + (cur ^ 1) * kFootBuf, &tma_bars[g][cur ^ 1]);
+        inflight |= 2u >> cur;
+      }
       pb ^= 1;
     }
     CornerMasks& cm = masks_s[g];
     if (staged) {
-      ptx::cp_async_wait<1>();  // this unit's copies (all but the group just committed)
-      if (s.noise) stage_noise<SH>(L, f0, f1, foot, gt);
+      // this unit's boxes (bounded wait; a timeout is reported and the unit's results discarded)
+      if (ptx::mbar_wait(&tma_bars[g][cur], (tph >> cur) & 1u)) {
+        tph ^= 1u << cur;
+        inflight &= ~(1u << cur);
+      } else {
+        atomicExch(&fail_s, 1);  // still in flight: waited for again before exit
+      }
+      if (s.noise) stage_noise<SH>(L, boxes, f0, f1, foot, gt);
       for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) {
         uint32_t* m = i < 2 * kMaxBoxW ? &cm.xlo[0][0] + i
                       : i < 4 * kMaxBoxW ? &cm.xhi[0][0] + (i - 2 * kMaxBoxW)
@@ -708,13 +711,13 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       bar_group(g);
       build_masks(s, L.d0, L.d1, f0, f1, unit, cm, gt);
     }
-    gather_half<SH>(L, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
+    gather_half<SH>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < Kp / 16; k++)
-        ptx::mma_bf16(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_M128_N64_K, k > 0);
+        ptx::mma_bf16(win, dXk.at(k * 256), dW0k.at(k * 256), I_M128_N64_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -733,7 +736,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, ptx::desc(aP0 + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_M128_N64_K, k > 0);
+        ptx::mma_bf16(win, dP0k.at(k * 256), dW1k.at(k * 256), I_M128_N64_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -750,8 +753,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win + 64, ptx::desc(aP1 + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_M128_N16_K,
-                      k > 0);
+        ptx::mma_bf16(win + 64, dP1k.at(k * 256), dWok.at(k * 256), I_M128_N16_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -777,11 +779,11 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (issuer) {
       ptx::fence_after_sync();
       // dA1 = dY Wout: B = Wout viewed [c][h] as MN-major (N = h)
-      ptx::mma_bf16(win, ptx::desc(adY, 128, S16), ptx::desc(aWo, S64, 128), I_M128_N64_BMN, 0);
+      ptx::mma_bf16(win, ptx::desc_base(adY, 128, S16).at(0), ptx::desc_base(aWo, S64, 128).at(0), I_M128_N64_BMN, 0);
       // dWout^T += A1^T dY : A = A1 (M = h), B = dY (N = c), K = texels
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColWo, ptx::desc(aP1 + k * 2 * S64, S64, 128), ptx::desc(adY + k * 2 * S16, S16, 128),
+        ptx::mma_bf16(tbase + kColWo, dP1m.at(k * 2 * S64), dYm.at(k * 2 * S16),
                       I_M64_N16_MN, 1);
       ptx::commit(bar);
     }
@@ -803,12 +805,12 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       // dA0 = dH1 W1 : B = W1 viewed [i][h] as MN-major (N = h), K = i
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, ptx::desc(aP1 + k * 256, 128, S64), ptx::desc(aW1 + k * 2 * S64, S64, 128), I_M128_N64_BMN,
+        ptx::mma_bf16(win, dP1k.at(k * 256), dW1m.at(k * 2 * S64), I_M128_N64_BMN,
                       k > 0);
       // dW1 += dH1^T A0
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW1, ptx::desc(aP1 + k * 2 * S64, S64, 128), ptx::desc(aP0 + k * 2 * S64, S64, 128),
+        ptx::mma_bf16(tbase + kColW1, dP1m.at(k * 2 * S64), dP0m.at(k * 2 * S64),
                       I_M64_N64_MN, 1);
       ptx::commit(bar);
     }
@@ -830,12 +832,12 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       // dX = dH0 W0 : B = W0 viewed [h][f] as MN-major (N = f), K = h
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, ptx::desc(aP0 + k * 256, 128, S64), ptx::desc(aW0 + k * 2 * SX, SX, 128), I_M128_NKP_BMN,
+        ptx::mma_bf16(win, dP0k.at(k * 256), dW0m.at(k * 2 * SX), I_M128_NKP_BMN,
                       k > 0);
       // dW0 += dH0^T X
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW0, ptx::desc(aP0 + k * 2 * S64, S64, 128), ptx::desc(aX + k * 2 * SX, SX, 128),
+        ptx::mma_bf16(tbase + kColW0, dP0m.at(k * 2 * S64), dXm.at(k * 2 * SX),
                       I_M64_NKP_MN, 1);
       ptx::commit(bar);
     }
@@ -933,7 +935,11 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     bar_group(g);
   }
 
-  ptx::cp_async_wait<0>();  // no copy may still target shared memory at exit
+  // no load may still target shared memory at exit (loads in flight only after an early exit)
+  for (int b = 0; b < 2; b++)
+    if (inflight & (1u << b)) {
+      if (!ptx::mbar_wait(&tma_bars[g][b], (tph >> b) & 1u)) atomicExch(&fail_s, 1);
+    }
 
   // ------------------------------------------------------------------ weight gradients out
   const double ls = block_sum_d_tc(loss, red);
@@ -976,13 +982,13 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
 template <class SH>
 cudaError_t launch_shape(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                         cudaStream_t stream)
+                         const LatentBoxes& boxes, cudaStream_t stream)
 {
   constexpr size_t smem = smem_bytes<SH>();
   static_assert(smem <= 227 * 1024, "shared memory budget");
   cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tc_unit_kernel<SH><<<grid, kThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error);
+  tc_unit_kernel<SH><<<grid, kThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error, boxes);
   return cudaGetLastError();
 }
 
@@ -997,18 +1003,20 @@ int tc_max_grid()
 }
 
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                            cudaStream_t stream)
+                            const LatentBoxes& boxes, cudaStream_t stream)
 {
   // profile shapes (libopenntc.cpp:289-333): C0, C1, padded feature dim
   if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64)
-    return launch_shape<Shape<8, 12, 64>>(M, d_steps, step_idx, grid, out, d_error, stream);
+    return launch_shape<Shape<8, 12, 64>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
   if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96)
-    return launch_shape<Shape<12, 20, 96>>(M, d_steps, step_idx, grid, out, d_error, stream);
+    return launch_shape<Shape<12, 20, 96>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
   if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80)
-    return launch_shape<Shape<12, 10, 80>>(M, d_steps, step_idx, grid, out, d_error, stream);
+    return launch_shape<Shape<12, 10, 80>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
   if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96)
-    return launch_shape<Shape<16, 12, 96>>(M, d_steps, step_idx, grid, out, d_error, stream);
+    return launch_shape<Shape<16, 12, 96>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
   return cudaErrorNotSupported;
 }
+
+int tc_box_capacity() { return kFootBuf; }
 
 }  // namespace ontc
