@@ -61,8 +61,11 @@ enum { ONTC_MANIFEST_LOADED = 0, ONTC_TRAIN_IN_PROGRESS = 1, ONTC_TRAIN_COMPLETE
  * cuBLAS TF32, libopenntc.cpp:374).
  *   BF16 (default): tcgen05/TMEM bf16 operands, fp32 accumulate, fp32 master weights and
  *                   fp32 Adam moments.
- *   FP32:           SIMT fp32 tile kernel (the plain comparator). */
-enum { ONTC_PRECISION_BF16 = 0, ONTC_PRECISION_FP32 = 1 };
+ *   FP32:           SIMT fp32 tile kernel (exact fp32 products).
+ *   BF16X3:         tcgen05 products of fp32 operands split into bf16 high and low parts
+ *                   (h.h + h.l + l.h, three bf16 MMAs, fp32 accumulate), fp32 activations:
+ *                   about 16 mantissa bits per product, more than upstream's tf32 products. */
+enum { ONTC_PRECISION_BF16 = 0, ONTC_PRECISION_FP32 = 1, ONTC_PRECISION_BF16X3 = 2 };
 
 /* Decoder arithmetic for ontc_decode (upstream: HLSL only, ntc_decode.hlsli:605-623). */
 enum {
@@ -376,7 +379,8 @@ enum {
   ONTC_KCLASS_CATCHUP = 3,    /* deferred optimiser: footprint catch-up and level sweeps */
   ONTC_KCLASS_SIDE_CATCHUP = 4, /* the next step's catch-up, on the side stream beside a tile kernel */
   ONTC_KCLASS_SIDE_UPDATE = 5,  /* a step's footprint update outside the next footprint, side stream */
-  ONTC_KCLASS_COUNT = 6
+  ONTC_KCLASS_UNITS_BF16X3 = 6, /* the tile kernel, tcgen05 split-bf16 (BF16X3) */
+  ONTC_KCLASS_COUNT = 7
 };
 typedef struct ontc_kernel_time {
   int64_t launches;

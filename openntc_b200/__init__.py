@@ -68,6 +68,7 @@ class TrainPhase(enum.IntEnum):
 class Precision(enum.IntEnum):
     BF16 = 0
     FP32 = 1
+    BF16X3 = 2
 
 
 class LatentAdam(enum.IntEnum):

@@ -21,7 +21,7 @@ RESULT_NAMES = ["Success", "InvalidDimension", "AllocationFailure", "InvalidMani
 BPP_0_2, BPP_0_5, BPP_1_0, BPP_2_25 = range(4)
 QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH, QUALITY_ULTRA = range(4)
 MANIFEST_LOADED, TRAIN_IN_PROGRESS, TRAIN_COMPLETE, TRAIN_ERROR = 0, 1, 2, -1
-PRECISION_BF16, PRECISION_FP32 = 0, 1
+PRECISION_BF16, PRECISION_FP32, PRECISION_BF16X3 = 0, 1, 2
 DECODE_INT8 = 0  # ONTC_DECODE_INT8: SampleMaterial integer semantics
 DECODE_FP32, DECODE_BF16, DECODE_FP8 = 1, 2, 3  # float-model decoders (ontc_decoder_create_float)
 SCREEN_DISCARD_OUTSIDE = 1  # ONTC_SCREEN_DISCARD_OUTSIDE
@@ -99,7 +99,7 @@ class KernelTime(C.Structure):
 
 
 KCLASS_UNITS_FP32, KCLASS_UNITS_BF16, KCLASS_ADAM, KCLASS_CATCHUP = 0, 1, 2, 3
-KCLASS_SIDE_CATCHUP, KCLASS_SIDE_UPDATE, KCLASS_COUNT = 4, 5, 6
+KCLASS_SIDE_CATCHUP, KCLASS_SIDE_UPDATE, KCLASS_UNITS_BF16X3, KCLASS_COUNT = 4, 5, 6, 7
 
 
 class DebugStep(C.Structure):

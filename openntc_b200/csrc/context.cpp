@@ -1266,7 +1266,8 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
 int ontc_set_train_options(ontc_context* c, const ontc_train_options* o)
 {
   if (!c->initialized || !o) return ONTC_INVALID_STATE;
-  if (o->precision != ONTC_PRECISION_FP32 && o->precision != ONTC_PRECISION_BF16) return ONTC_INVALID_STATE;
+  if (o->precision != ONTC_PRECISION_FP32 && o->precision != ONTC_PRECISION_BF16 && o->precision != ONTC_PRECISION_BF16X3)
+    return ONTC_INVALID_STATE;
   if (c->batch_i > 0) return ONTC_INVALID_STATE;
   if (o->noise_mode != ONTC_NOISE_COUNTER && o->noise_mode != ONTC_NOISE_UPSTREAM) return ONTC_INVALID_STATE;
   if (o->latent_adam != ONTC_LATENT_ADAM_DEFERRED && o->latent_adam != ONTC_LATENT_ADAM_DENSE) return ONTC_INVALID_STATE;
@@ -1513,10 +1514,12 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       int cls = ONTC_KCLASS_UNITS_FP32;
       c->prof_begin();
       if (e) {
-      } else if (c->precision == ONTC_PRECISION_BF16) {
-        grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
-        cls = ONTC_KCLASS_UNITS_BF16;
-        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->boxes[s.lod], c->stream);
+      } else if (c->precision == ONTC_PRECISION_BF16 || c->precision == ONTC_PRECISION_BF16X3) {
+        const bool split = c->precision == ONTC_PRECISION_BF16X3;
+        const int gpc = tc_groups_per_cta(split);  // work units in flight per CTA
+        grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
+        cls = split ? ONTC_KCLASS_UNITS_BF16X3 : ONTC_KCLASS_UNITS_BF16;
+        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->boxes[s.lod], split, c->stream);
         if (e == cudaErrorNotSupported) {
           cudaGetLastError();
           grid = std::min(units, c->sms);
@@ -1960,9 +1963,11 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
   const Model M = c->model();
   TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
   if (!e) {
-    if (c->precision == ONTC_PRECISION_BF16) {
-      grid = std::min((units + 1) / 2, tc_max_grid());  // two work units in flight per CTA
-      e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->boxes[s.lod], c->stream);
+    if (c->precision == ONTC_PRECISION_BF16 || c->precision == ONTC_PRECISION_BF16X3) {
+      const bool split = c->precision == ONTC_PRECISION_BF16X3;
+      const int gpc = tc_groups_per_cta(split);
+      grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
+      e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->boxes[s.lod], split, c->stream);
       if (e == cudaErrorNotSupported) {
         cudaGetLastError();
         grid = std::min(units, c->sms);

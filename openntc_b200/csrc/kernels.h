@@ -115,9 +115,12 @@ cudaError_t make_latent_boxes(const float* p0, const float* p1, int d0, int d1, 
 size_t simt_smem_bytes(int F);
 cudaError_t launch_simt_units(int mode, const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
                               cudaStream_t stream);
-// BF16 tcgen05 path; returns cudaErrorNotSupported when the profile has no tcgen05 variant
+// tcgen05 tile kernel, bf16 operands or (split) fp32 operands as bf16 high + low parts; returns
+// cudaErrorNotSupported when the profile has no tcgen05 variant
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
-                            int* d_error, const LatentBoxes& boxes, cudaStream_t stream);
+                            int* d_error, const LatentBoxes& boxes, bool split, cudaStream_t stream);
+// 128-texel units a tile CTA works on at once (its grid: units / this, at most one CTA per SM)
+int tc_groups_per_cta(bool split);
 // the staging buffer the tile kernel gives a unit's latent boxes, in floats
 int tc_box_capacity();
 int tc_max_grid();

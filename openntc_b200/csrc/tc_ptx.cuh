@@ -164,6 +164,13 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn, bool 
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor with fp32 D: A/B format `fmt` (kind::f16: 0 f16, 1 bf16).
+__host__ __device__ constexpr uint32_t idesc_f32acc(uint32_t fmt, int M, int N, bool a_mn, bool b_mn)
+{
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // Instruction descriptor, kind::i8 with signed int8 A/B and s32 D.
 __host__ __device__ constexpr uint32_t idesc_s8(int M, int N, bool a_mn, bool b_mn)
 {

@@ -34,7 +34,6 @@ namespace ontc {
 
 namespace {
 
-constexpr int kThreads = 512;      // 2 groups x 256
 constexpr int kGroupThreads = 256; // 2 threads per texel row: half 0 / half 1 of the columns
 constexpr uint32_t kTmemCols = 512;
 // TMEM column map: per group a 128-column window [128 g, 128 g + 128) holding
@@ -48,26 +47,51 @@ constexpr int kFootBuf = kFootFloats / 2;
 constexpr int kMaxBoxW = 64;       // latent box limits of the owner-computes scatter
 constexpr int kMaxBoxH = 32;
 
+// Operand tiles of the MMAs, all bf16 (tcgen05 kind::f16, fp32 accumulate).
+//   EBf16:  one bf16 tile per operand; two 8-warp groups per CTA.
+//   ESplit: each fp32 operand value v kept as a bf16 high part h = bf16(v) and low part
+//           l = bf16(v - h) in two tiles (the low tile right after the high one), and each
+//           product formed as h.h + h.l + l.h by three MMAs into the same fp32 accumulator:
+//           about 16 mantissa bits per product, more than the tf32 products of upstream's
+//           cuBLAS GEMMs (libopenntc.cpp:374).  Its tiles are twice as large: one group per CTA.
+// (kind::tf32 itself reads MN-major operands only in a 32-byte-granule 128-byte swizzle, which
+// the same tile cannot share with its K-major use in the next layer.)
+struct EBf16 {
+  static constexpr bool kSplit = false;
+  static constexpr int kGroups = 2, kTileMul = 1;
+};
+struct ESplit {
+  static constexpr bool kSplit = true;
+  static constexpr int kGroups = 1, kTileMul = 2;
+};
+// byte stride between 8-row groups of a [*][cols] bf16 operand tile in the canonical layout
+constexpr uint32_t row8(int cols) { return (uint32_t)(cols / 8) * 128; }
+
 template <int C0_, int C1_, int KP_>
 struct Shape {
   static constexpr int C0 = C0_, C1 = C1_, Kp = KP_;
   static constexpr int F = ((4 * C0 + C1 + 13 + 3) / 4) * 4;
-  static constexpr uint32_t SX = (Kp / 8) * 128;  // 8-row group stride of a [*][Kp] tile
 };
 
-constexpr uint32_t S64 = 8 * 128;  // 8-row group stride of a [*][64] tile
-constexpr uint32_t S16 = 2 * 128;  // ... of a [*][16] tile
+// a [rows][cols] operand tile: the bf16 tile and, split, its low-part tile after it
+template <class E>
+constexpr uint32_t tile_bytes(int rows, int cols)
+{
+  return (uint32_t)(rows * cols * 2 * E::kTileMul);
+}
 
-template <class SH>
+template <class SH, class E>
 struct GroupSmem {
-  static constexpr size_t kX = 128 * SH::Kp * 2, kP = 128 * 64 * 2, kY = 128 * 16 * 2, kFoot = kFootFloats * 4;
+  static constexpr size_t kX = tile_bytes<E>(128, SH::Kp), kP = tile_bytes<E>(128, 64), kY = tile_bytes<E>(128, 16);
+  static constexpr size_t kFoot = kFootFloats * 4;
   static constexpr size_t kBytes = kX + 2 * kP + kY + kFoot;
 };
 
-template <class SH>
+template <class SH, class E>
 constexpr size_t smem_bytes()
 {
-  return 2 * GroupSmem<SH>::kBytes + 64 * SH::Kp * 2 + 64 * 64 * 2 + 16 * 64 * 2 + 1024;
+  return E::kGroups * GroupSmem<SH, E>::kBytes + tile_bytes<E>(64, SH::Kp) + tile_bytes<E>(64, 64) +
+         tile_bytes<E>(16, 64) + 1024;
 }
 
 struct GroupPtrs {
@@ -84,15 +108,63 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// Stores 8 consecutive values (columns c0..c0+7, c0 % 8 == 0) of row r as one 16-byte chunk.
-__device__ __forceinline__ void st_chunk(uint8_t* base, int r, int c0, int cols, const float* v)
+// Stores 8 consecutive values (columns c0..c0+7, c0 % 8 == 0) of row r of a [rows][cols]
+// operand tile as one 16-byte bf16 chunk; split, also their low parts in the low-part tile.
+template <class E>
+__device__ __forceinline__ void st_chunk(uint8_t* base, int r, int c0, int rows, int cols, const float* v)
 {
   uint4 q;
   q.x = pack_bf16(v[0], v[1]);
   q.y = pack_bf16(v[2], v[3]);
   q.z = pack_bf16(v[4], v[5]);
   q.w = pack_bf16(v[6], v[7]);
-  *reinterpret_cast<uint4*>(base + ptx::cm_off16(r, c0, cols)) = q;
+  const uint32_t off = ptx::cm_off16(r, c0, cols);
+  *reinterpret_cast<uint4*>(base + off) = q;
+  if constexpr (E::kSplit) {
+    const uint32_t* h = &q.x;
+    float lo[8];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const __nv_bfloat162 hb = *reinterpret_cast<const __nv_bfloat162*>(&h[i]);
+      lo[2 * i] = v[2 * i] - __low2float(hb);  // exact: the high part is v rounded to bf16
+      lo[2 * i + 1] = v[2 * i + 1] - __high2float(hb);
+    }
+    uint4 l;
+    l.x = pack_bf16(lo[0], lo[1]);
+    l.y = pack_bf16(lo[2], lo[3]);
+    l.z = pack_bf16(lo[4], lo[5]);
+    l.w = pack_bf16(lo[6], lo[7]);
+    *reinterpret_cast<uint4*>(base + rows * cols * 2 + off) = l;
+  }
+}
+
+// D (+)= A B, operands given by descriptor bases and byte offsets; split, the low parts of A and
+// B lie a_lo / b_lo bytes after the high ones and D += A.h B.h + A.h B.l + A.l B.h
+template <class E>
+__device__ __forceinline__ void mma(uint32_t d, const ptx::DescBase& A, uint32_t a_off, uint32_t a_lo,
+                                    const ptx::DescBase& B, uint32_t b_off, uint32_t b_lo, uint32_t idesc,
+                                    uint32_t acc)
+{
+  ptx::mma_bf16(d, A.at(a_off), B.at(b_off), idesc, acc);
+  if constexpr (E::kSplit) {
+    ptx::mma_bf16(d, A.at(a_off), B.at(b_off + b_lo), idesc, 1);
+    ptx::mma_bf16(d, A.at(a_off + a_lo), B.at(b_off), idesc, 1);
+  }
+}
+
+// upstream's hardgelu and its derivative in fp32 (the split epilogues), as 8-column chunks
+__device__ __forceinline__ void hg_chunk_f32(const float* x, float* a, uint32_t* pre)
+{
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    pre[i] = __float_as_uint(x[i]);
+    a[i] = hardgelu(x[i]);
+  }
+}
+__device__ __forceinline__ void dhg_chunk_f32(const float* da, const uint32_t* pre, float* d)
+{
+#pragma unroll
+  for (int i = 0; i < 8; i++) d[i] = da[i] * hardgelu_grad(__uint_as_float(pre[i]));
 }
 
 __device__ __forceinline__ void bar_group(int g) { asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kGroupThreads) : "memory"); }
@@ -342,7 +414,7 @@ struct RowWriter {
 // 4 C0 g0 corner features, half 1 the C1 bilinear g1 features, positional encoding, lod and
 // padding.  `staged`: the latents (noise already added) come from the shared-memory boxes.
 // Otherwise gather_half_direct reads them, and adds the noise, from global memory.
-template <class SH>
+template <class SH, class E>
 __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int row, int half, uint8_t* sX)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
@@ -355,7 +427,7 @@ __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int r
   auto put = [&](float v) {
     buf[f & 7] = v;
     f++;
-    if ((f & 7) == 0) st_chunk(sX, row, col0 + f - 8, Kp, buf);
+    if ((f & 7) == 0) st_chunk<E>(sX, row, col0 + f - 8, 128, Kp, buf);
   };
   if (half == 0) {
 #pragma unroll
@@ -385,7 +457,7 @@ __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int r
   for (int i = 4 * C0 + C1 + 13; i < Kp; i++) put(0.0f);
 }
 
-template <class SH>
+template <class SH, class E>
 __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxes& B, int x, int y, bool valid, int row,
                                            int half, bool staged, const Foot& f0, const Foot& f1, const float* foot,
                                            uint8_t* sX)
@@ -396,11 +468,11 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxe
   const int col0 = half ? kSplit : 0, col1 = half ? Kp : kSplit;
   if (!valid) {
     const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = col0; c < col1; c += 8) st_chunk(sX, row, c, Kp, z);
+    for (int c = col0; c < col1; c += 8) st_chunk<E>(sX, row, c, 128, Kp, z);
     return;
   }
   if (!staged) {
-    gather_half_direct<SH>(L, x, y, row, half, sX);
+    gather_half_direct<SH, E>(L, x, y, row, half, sX);
     return;
   }
   const int d0 = L.d0, d1 = L.d1;
@@ -412,7 +484,7 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxe
   auto put = [&](float v) {
     buf[f & 7] = v;
     f++;
-    if ((f & 7) == 0) st_chunk(sX, row, col0 + f - 8, Kp, buf);
+    if ((f & 7) == 0) st_chunk<E>(sX, row, col0 + f - 8, 128, Kp, buf);
   };
   if (half == 0) {
 #pragma unroll
@@ -475,32 +547,66 @@ __device__ __noinline__ void scatter_direct(LevelArgs L, int x, int y, int half,
   }
 }
 
-// Loads the fp32 master weights into the bf16 canonical tiles (zero padding past F / C).
-template <class SH>
+// Loads the fp32 master weights into the canonical operand tiles (zero padding past F / C).
+template <class SH, class E>
 __device__ void load_weights(const Model& M, uint8_t* W0, uint8_t* W1, uint8_t* Wo)
 {
-  constexpr int F = SH::F, Kp = SH::Kp;
+  constexpr int F = SH::F, Kp = SH::Kp, kThreads = E::kGroups * kGroupThreads;
   const int C = M.C;
   for (int i = threadIdx.x; i < 64 * (Kp / 8); i += kThreads) {
     const int r = i / (Kp / 8), c0 = (i % (Kp / 8)) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = (c0 + j) < F ? M.W[w0_off() + r * F + c0 + j] : 0.0f;
-    st_chunk(W0, r, c0, Kp, v);
+    st_chunk<E>(W0, r, c0, 64, Kp, v);
   }
   for (int i = threadIdx.x; i < 64 * 8; i += kThreads) {
     const int r = i / 8, c0 = (i % 8) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = M.W[w1_off(F) + r * 64 + c0 + j];
-    st_chunk(W1, r, c0, 64, v);
+    st_chunk<E>(W1, r, c0, 64, 64, v);
   }
   for (int i = threadIdx.x; i < 16 * 8; i += kThreads) {
     const int r = i / 8, c0 = (i % 8) * 8;
     float v[8];
     for (int j = 0; j < 8; j++) v[j] = r < C ? M.W[wo_off(F) + r * 64 + c0 + j] : 0.0f;
-    st_chunk(Wo, r, c0, 64, v);
+    st_chunk<E>(Wo, r, c0, 16, 64, v);
   }
 }
 
+// Forward epilogue of one layer, this thread's 32 columns (from hc): activations into the next
+// operand tile P, pre-activations kept in `pre` (packed bf16 pairs, or fp32 bits) for the
+// backward pass.
+template <class E>
+__device__ __forceinline__ void epi_fwd(const float* hx, uint32_t* pre, uint8_t* P, int row, int hc)
+{
+#pragma unroll
+  for (int c = 0; c < 32; c += 8) {
+    if constexpr (!E::kSplit) {
+      *reinterpret_cast<uint4*>(P + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(hx + c, pre + c / 2);
+    } else {
+      float a[8];
+      hg_chunk_f32(hx + c, a, pre + c);
+      st_chunk<E>(P, row, hc + c, 128, 64, a);
+    }
+  }
+}
+// Backward epilogue: dA * hardgelu'(pre) for this thread's 32 columns into the operand tile P.
+template <class E>
+__device__ __forceinline__ void epi_bwd(const float* da, const uint32_t* pre, uint8_t* P, int row, int hc)
+{
+#pragma unroll
+  for (int c = 0; c < 32; c += 8) {
+    if constexpr (!E::kSplit) {
+      *reinterpret_cast<uint4*>(P + ptx::cm_off16(row, hc + c, 64)) = dhg_chunk_bf16(da + c, pre + c / 2);
+    } else {
+      float d[8];
+      dhg_chunk_f32(da + c, pre + c, d);
+      st_chunk<E>(P, row, hc + c, 128, 64, d);
+    }
+  }
+}
+
+template <int kThreads>
 __device__ __forceinline__ double block_sum_d_tc(double v, double* red)
 {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -523,13 +629,21 @@ __device__ __forceinline__ void tmem_st_zero16(uint32_t taddr)
       "r"(z));
 }
 
-template <class SH>
-__global__ void __launch_bounds__(kThreads, 1)
+template <class SH, class E>
+__global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1)
 tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut out, int* __restrict__ err,
                const __grid_constant__ LatentBoxes boxes)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp, F = SH::F;
-  constexpr uint32_t SX = SH::SX;
+  constexpr int kThreads = E::kGroups * kGroupThreads;
+  constexpr int kParts = E::kGroups * 2;  // splits of the per-CTA epilogue work
+  // 8-row group strides of the [*][Kp], [*][64] and [*][16] operand tiles
+  constexpr uint32_t SX = row8(Kp), S64 = row8(64), S16 = row8(16);
+  constexpr int kK = 16;         // K elements per bf16 MMA instruction
+  constexpr uint32_t kKS = 2;    // MN-major operands: 8-row groups per MMA K step
+  // bytes from a tile's high part to its low part (split operands)
+  constexpr uint32_t kLoX = 128 * Kp * 2, kLoP = 128 * 64 * 2, kLoY = 128 * 16 * 2;
+  constexpr uint32_t kLoW0 = 64 * Kp * 2, kLoW1 = 64 * 64 * 2, kLoWo = 16 * 64 * 2;
   constexpr int KH = Kp / 2;  // dX columns per half row (a multiple of 8)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
@@ -551,20 +665,21 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   const int gt = tid & 255;        // thread within the group
   const int row = gt & 127;        // texel row == TMEM lane
   const int half = gt >> 7;        // which half of the row's columns this thread takes
-  const int part = g * 2 + half;   // 0..3: splits the per-CTA epilogue work
+  const int part = g * 2 + half;   // 0 .. kParts - 1: splits the per-CTA epilogue work
   const int quad = warp & 3;       // TMEM lane quadrant this warp may access
   const int C = M.C;
 
-  uint8_t* base = smem_raw + g * GroupSmem<SH>::kBytes;
+  using GS = GroupSmem<SH, E>;
+  uint8_t* base = smem_raw + g * GS::kBytes;
   GroupPtrs gp;
   gp.X = base;
-  gp.P0 = gp.X + GroupSmem<SH>::kX;
-  gp.P1 = gp.P0 + GroupSmem<SH>::kP;
-  gp.dY = gp.P1 + GroupSmem<SH>::kP;
-  gp.foot = reinterpret_cast<float*>(gp.dY + GroupSmem<SH>::kY);
-  uint8_t* sW0 = smem_raw + 2 * GroupSmem<SH>::kBytes;
-  uint8_t* sW1 = sW0 + 64 * Kp * 2;
-  uint8_t* sWo = sW1 + 64 * 64 * 2;
+  gp.P0 = gp.X + GS::kX;
+  gp.P1 = gp.P0 + GS::kP;
+  gp.dY = gp.P1 + GS::kP;
+  gp.foot = reinterpret_cast<float*>(gp.dY + GS::kY);
+  uint8_t* sW0 = smem_raw + E::kGroups * GS::kBytes;
+  uint8_t* sW1 = sW0 + tile_bytes<E>(64, Kp);
+  uint8_t* sWo = sW1 + tile_bytes<E>(64, 64);
 
   if (tid == 0) {
     ptx::mbar_init(&bars[0], 1);
@@ -574,7 +689,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     fail_s = 0;
   }
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
-  load_weights<SH>(M, sW0, sW1, sWo);
+  load_weights<SH, E>(M, sW0, sW1, sWo);
   if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
   static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
   if (tid < (int)(sizeof(StepRec) / 4))
@@ -587,9 +702,10 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   const LevelArgs& L = level_s;
   const uint32_t tbase = tmem_base_s;
   const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
-  // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16): each of
-  // the 4 parts takes every 4th 16-column chunk of its quadrant's lanes
-  for (uint32_t c = kColW0 + 16 * (uint32_t)part; c < kColWo + 16; c += 64) tmem_st_zero16(tbase + lane_off + c);
+  // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16): each part
+  // takes every kParts-th 16-column chunk of its quadrant's lanes
+  for (uint32_t c = kColW0 + 16 * (uint32_t)part; c < kColWo + 16; c += 16 * kParts)
+    tmem_st_zero16(tbase + lane_off + c);
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   ptx::fence_before_sync();
   __syncthreads();
@@ -621,13 +737,14 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     bar_group(g);
   };
 
-  constexpr uint32_t I_M128_N64_K = ptx::idesc_bf16(128, 64, false, false);
-  constexpr uint32_t I_M128_N16_K = ptx::idesc_bf16(128, 16, false, false);
-  constexpr uint32_t I_M128_N64_BMN = ptx::idesc_bf16(128, 64, false, true);
-  constexpr uint32_t I_M128_NKP_BMN = ptx::idesc_bf16(128, Kp, false, true);
-  constexpr uint32_t I_M64_N16_MN = ptx::idesc_bf16(64, 16, true, true);
-  constexpr uint32_t I_M64_N64_MN = ptx::idesc_bf16(64, 64, true, true);
-  constexpr uint32_t I_M64_NKP_MN = ptx::idesc_bf16(64, Kp, true, true);
+  constexpr uint32_t FM = 1;  // bf16 operands
+  constexpr uint32_t I_M128_N64_K = ptx::idesc_f32acc(FM, 128, 64, false, false);
+  constexpr uint32_t I_M128_N16_K = ptx::idesc_f32acc(FM, 128, 16, false, false);
+  constexpr uint32_t I_M128_N64_BMN = ptx::idesc_f32acc(FM, 128, 64, false, true);
+  constexpr uint32_t I_M128_NKP_BMN = ptx::idesc_f32acc(FM, 128, Kp, false, true);
+  constexpr uint32_t I_M64_N16_MN = ptx::idesc_f32acc(FM, 64, 16, true, true);
+  constexpr uint32_t I_M64_N64_MN = ptx::idesc_f32acc(FM, 64, 64, true, true);
+  constexpr uint32_t I_M64_NKP_MN = ptx::idesc_f32acc(FM, 64, Kp, true, true);
   const uint32_t aX = ptx::smem_addr(gp.X), aP0 = ptx::smem_addr(gp.P0), aP1 = ptx::smem_addr(gp.P1);
   const uint32_t adY = ptx::smem_addr(gp.dY);
   const uint32_t aW0 = ptx::smem_addr(sW0), aW1 = ptx::smem_addr(sW1), aWo = ptx::smem_addr(sWo);
@@ -636,22 +753,22 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   const ptx::DescBase dXk = ptx::desc_base(aX, 128, SX), dXm = ptx::desc_base(aX, SX, 128);
   const ptx::DescBase dP0k = ptx::desc_base(aP0, 128, S64), dP0m = ptx::desc_base(aP0, S64, 128);
   const ptx::DescBase dP1k = ptx::desc_base(aP1, 128, S64), dP1m = ptx::desc_base(aP1, S64, 128);
-  const ptx::DescBase dYm = ptx::desc_base(adY, S16, 128);
+  const ptx::DescBase dYk = ptx::desc_base(adY, 128, S16), dYm = ptx::desc_base(adY, S16, 128);
   const ptx::DescBase dW0k = ptx::desc_base(aW0, 128, SX), dW0m = ptx::desc_base(aW0, SX, 128);
   const ptx::DescBase dW1k = ptx::desc_base(aW1, 128, S64), dW1m = ptx::desc_base(aW1, S64, 128);
-  const ptx::DescBase dWok = ptx::desc_base(aWo, 128, S64);
+  const ptx::DescBase dWok = ptx::desc_base(aWo, 128, S64), dWom = ptx::desc_base(aWo, S64, 128);
   const int hc = half * 32;  // this thread's first column of a 64-column tile
 
   // latent boxes: unit k's were loaded (TMA, asynchronously) while unit k-1 ran, into the
   // staging buffer the previous unit did not use; tph holds each buffer's next wait parity and
   // inflight which buffers have loads not yet waited for
-  const int ustride = gridDim.x * 2;
+  const int ustride = gridDim.x * E::kGroups;
   Foot nf0 = {}, nf1 = {};
   bool nstaged = false;
   int pb = 0;
   uint32_t tph = 0, inflight = 0;
   {
-    const int u0 = blockIdx.x * 2 + g;
+    const int u0 = blockIdx.x * E::kGroups + g;
     nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
     if (nstaged) {
       if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
@@ -659,7 +776,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     }
   }
 
-  for (int unit = blockIdx.x * 2 + g; unit < ntiles; unit += ustride) {
+  for (int unit = blockIdx.x * E::kGroups + g; unit < ntiles; unit += ustride) {
     // ------------------------------------------------------------------ gather
     const int b = unit * kTile + row;
     const bool valid = b < s.texels;
@@ -711,32 +828,29 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       bar_group(g);
       build_masks(s, L.d0, L.d1, f0, f1, unit, cm, gt);
     }
-    gather_half<SH>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
+    gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
-      for (int k = 0; k < Kp / 16; k++)
-        ptx::mma_bf16(win, dXk.at(k * 256), dW0k.at(k * 256), I_M128_N64_K, k > 0);
+      for (int k = 0; k < Kp / kK; k++) mma<E>(win, dXk, k * 256, kLoX, dW0k, k * 256, kLoW0, I_M128_N64_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 0 epilogue
-    uint32_t h0[16], h1[16];  // pre-activations of this thread's 32 columns, packed bf16 pairs
+    constexpr int kPre = E::kSplit ? 32 : 16;
+    uint32_t h0[kPre], h1[kPre];  // pre-activations of this thread's 32 columns (bf16 pairs or fp32)
     float hx[32];
     ptx::ld16(lwin + hc, hx);
     ptx::ld16(lwin + hc + 16, hx + 16);
     ptx::ld_wait();
-#pragma unroll
-    for (int c = 0; c < 32; c += 8)
-      *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(hx + c, h0 + c / 2);
+    epi_fwd<E>(hx, h0, gp.P0, row, hc);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, dP0k.at(k * 256), dW1k.at(k * 256), I_M128_N64_K, k > 0);
+      for (int k = 0; k < 64 / kK; k++) mma<E>(win, dP0k, k * 256, kLoP, dW1k, k * 256, kLoW1, I_M128_N64_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -745,15 +859,13 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     ptx::ld16(lwin + hc, hx);
     ptx::ld16(lwin + hc + 16, hx + 16);
     ptx::ld_wait();
-#pragma unroll
-    for (int c = 0; c < 32; c += 8)
-      *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = hg_chunk_bf16(hx + c, h1 + c / 2);
+    epi_fwd<E>(hx, h1, gp.P1, row, hc);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win + 64, dP1k.at(k * 256), dWok.at(k * 256), I_M128_N16_K, k > 0);
+      for (int k = 0; k < 64 / kK; k++)
+        mma<E>(win + 64, dP1k, k * 256, kLoP, dWok, k * 256, kLoWo, I_M128_N16_K, k > 0);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -773,18 +885,19 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
           d[j] = inv * r;
         }
       }
-      st_chunk(gp.dY, row, half * 8, 16, d);
+      st_chunk<E>(gp.dY, row, half * 8, 128, 16, d);
     }
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
-      // dA1 = dY Wout: B = Wout viewed [c][h] as MN-major (N = h)
-      ptx::mma_bf16(win, ptx::desc_base(adY, 128, S16).at(0), ptx::desc_base(aWo, S64, 128).at(0), I_M128_N64_BMN, 0);
+      // dA1 = dY Wout: B = Wout viewed [c][h] as MN-major (N = h), K = c
+#pragma unroll
+      for (int k = 0; k < 16 / kK; k++)
+        mma<E>(win, dYk, k * 256, kLoY, dWom, k * kKS * S64, kLoWo, I_M128_N64_BMN, k > 0);
       // dWout^T += A1^T dY : A = A1 (M = h), B = dY (N = c), K = texels
 #pragma unroll
-      for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColWo, dP1m.at(k * 2 * S64), dYm.at(k * 2 * S16),
-                      I_M64_N16_MN, 1);
+      for (int k = 0; k < 128 / kK; k++)
+        mma<E>(tbase + kColWo, dP1m, k * kKS * S64, kLoP, dYm, k * kKS * S16, kLoY, I_M64_N16_MN, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -795,23 +908,19 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::ld16(lwin + hc, da);
       ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
-#pragma unroll
-      for (int c = 0; c < 32; c += 8)
-        *reinterpret_cast<uint4*>(gp.P1 + ptx::cm_off16(row, hc + c, 64)) = dhg_chunk_bf16(da + c, h1 + c / 2);
+      epi_bwd<E>(da, h1, gp.P1, row, hc);
     }
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
       // dA0 = dH1 W1 : B = W1 viewed [i][h] as MN-major (N = h), K = i
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, dP1k.at(k * 256), dW1m.at(k * 2 * S64), I_M128_N64_BMN,
-                      k > 0);
+      for (int k = 0; k < 64 / kK; k++)
+        mma<E>(win, dP1k, k * 256, kLoP, dW1m, k * kKS * S64, kLoW1, I_M128_N64_BMN, k > 0);
       // dW1 += dH1^T A0
 #pragma unroll
-      for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW1, dP1m.at(k * 2 * S64), dP0m.at(k * 2 * S64),
-                      I_M64_N64_MN, 1);
+      for (int k = 0; k < 128 / kK; k++)
+        mma<E>(tbase + kColW1, dP1m, k * kKS * S64, kLoP, dP0m, k * kKS * S64, kLoP, I_M64_N64_MN, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -822,23 +931,19 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::ld16(lwin + hc, da);
       ptx::ld16(lwin + hc + 16, da + 16);
       ptx::ld_wait();
-#pragma unroll
-      for (int c = 0; c < 32; c += 8)
-        *reinterpret_cast<uint4*>(gp.P0 + ptx::cm_off16(row, hc + c, 64)) = dhg_chunk_bf16(da + c, h0 + c / 2);
+      epi_bwd<E>(da, h0, gp.P0, row, hc);
     }
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
       // dX = dH0 W0 : B = W0 viewed [h][f] as MN-major (N = f), K = h
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        ptx::mma_bf16(win, dP0k.at(k * 256), dW0m.at(k * 2 * SX), I_M128_NKP_BMN,
-                      k > 0);
+      for (int k = 0; k < 64 / kK; k++)
+        mma<E>(win, dP0k, k * 256, kLoP, dW0m, k * kKS * SX, kLoW0, I_M128_NKP_BMN, k > 0);
       // dW0 += dH0^T X
 #pragma unroll
-      for (int k = 0; k < 8; k++)
-        ptx::mma_bf16(tbase + kColW0, dP0m.at(k * 2 * S64), dXm.at(k * 2 * SX),
-                      I_M64_NKP_MN, 1);
+      for (int k = 0; k < 128 / kK; k++)
+        mma<E>(tbase + kColW0, dP0m, k * kKS * S64, kLoP, dXm, k * kKS * SX, kLoX, I_M64_NKP_MN, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -942,7 +1047,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     }
 
   // ------------------------------------------------------------------ weight gradients out
-  const double ls = block_sum_d_tc(loss, red);
+  const double ls = block_sum_d_tc<kThreads>(loss, red);
   if (tid == 0) out.loss_partial[blockIdx.x] = ls;
   ptx::fence_after_sync();
   if (*(volatile int*)&fail_s == 0) {
@@ -950,7 +1055,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     const int lane = tid & 31;
     const int h = quad * 16 + lane;  // M=64 accumulators: row = lane of the quadrant's first 16
     const uint32_t la = tbase + lane_off;
-    for (int c = part * 8; c < Kp; c += 32) {  // dW0 [64][F], 8-column steps split by part
+    for (int c = part * 8; c < Kp; c += 8 * kParts) {  // dW0 [64][F], 8-column steps split by part
       float v[8];
       ptx::ld8(la + kColW0 + c, v);
       ptx::ld_wait();
@@ -958,19 +1063,19 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         for (int j = 0; j < 8; j++)
           if (c + j < F) dst[w0_off() + h * F + c + j] = v[j];
     }
-    {
-      float v[16];  // dW1[i][h]: accumulator row i, columns h, 16 per part
-      ptx::ld16(la + kColW1 + part * 16, v);
+    for (int c = part * 16; c < 64; c += 16 * kParts) {
+      float v[16];  // dW1[i][h]: accumulator row i, columns h, 16 per step
+      ptx::ld16(la + kColW1 + c, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 16; j++) dst[w1_off(F) + h * 64 + part * 16 + j] = v[j];
+        for (int j = 0; j < 16; j++) dst[w1_off(F) + h * 64 + c + j] = v[j];
     }
-    if (half == 0) {
+    for (int c = part * 8; c < 16; c += 8 * kParts) {
       float v[8];  // dWout^T[h][c] -> dWout[c][h]
-      ptx::ld8(la + kColWo + g * 8, v);
+      ptx::ld8(la + kColWo + c, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 8; j++) dst[wo_off(F) + (g * 8 + j) * 64 + h] = v[j];
+        for (int j = 0; j < 8; j++) dst[wo_off(F) + (c + j) * 64 + h] = v[j];
     }
   } else if (tid == 0) {
     atomicExch(err, 1);
@@ -980,16 +1085,32 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (warp == 0) ptx::tmem_dealloc(tbase, kTmemCols);
 }
 
-template <class SH>
+template <class SH, class E>
 cudaError_t launch_shape(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
                          const LatentBoxes& boxes, cudaStream_t stream)
 {
-  constexpr size_t smem = smem_bytes<SH>();
-  static_assert(smem <= 227 * 1024, "shared memory budget");
-  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  constexpr size_t smem = smem_bytes<SH, E>();
+  static_assert(smem <= 227 * 1024 - 6 * 1024, "shared memory budget (dynamic + static)");
+  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tc_unit_kernel<SH><<<grid, kThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error, boxes);
+  tc_unit_kernel<SH, E><<<grid, E::kGroups * kGroupThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error, boxes);
   return cudaGetLastError();
+}
+
+template <class E>
+cudaError_t launch_elem(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
+                        const LatentBoxes& boxes, cudaStream_t stream)
+{
+  // profile shapes (libopenntc.cpp:289-333): C0, C1, padded feature dim
+  if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64)
+    return launch_shape<Shape<8, 12, 64>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96)
+    return launch_shape<Shape<12, 20, 96>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80)
+    return launch_shape<Shape<12, 10, 80>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96)
+    return launch_shape<Shape<16, 12, 96>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  return cudaErrorNotSupported;
 }
 
 }  // namespace
@@ -1003,19 +1124,13 @@ int tc_max_grid()
 }
 
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                            const LatentBoxes& boxes, cudaStream_t stream)
+                            const LatentBoxes& boxes, bool split, cudaStream_t stream)
 {
-  // profile shapes (libopenntc.cpp:289-333): C0, C1, padded feature dim
-  if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64)
-    return launch_shape<Shape<8, 12, 64>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96)
-    return launch_shape<Shape<12, 20, 96>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80)
-    return launch_shape<Shape<12, 10, 80>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96)
-    return launch_shape<Shape<16, 12, 96>>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  return cudaErrorNotSupported;
+  return split ? launch_elem<ESplit>(M, d_steps, step_idx, grid, out, d_error, boxes, stream)
+              : launch_elem<EBf16>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
 }
+
+int tc_groups_per_cta(bool split) { return split ? ESplit::kGroups : EBf16::kGroups; }
 
 int tc_box_capacity() { return kFootBuf; }
 

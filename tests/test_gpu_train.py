@@ -157,7 +157,7 @@ def test_upstream_noise_buffers_match(materials, upstream_cls):
         ref.close()
 
 
-@pytest.mark.parametrize("precision", [ont.Precision.FP32, ont.Precision.BF16])
+@pytest.mark.parametrize("precision", [ont.Precision.FP32, ont.Precision.BF16, ont.Precision.BF16X3])
 def test_psnr_matches_upstream_at_equal_steps(materials, upstream_cls, precision):
     """Same seed, draws, init and (parity-mode) noise: final PSNR within 0.1 dB of upstream."""
     profile, steps, grids = ont.Profile.Bpp_0_5, 1000, 1
