@@ -13,8 +13,9 @@
 //   out  = saturate(acc2 * so)               -> global [n][C] f32
 //
 // The int8 products and int32 sums are exact, so the tensor cores reproduce the DP4A dot
-// products bit for bit; every float operation of the epilogues is written with explicit
-// round-to-nearest intrinsics in upstream's order, so outputs are bit-identical to the
+// products bit for bit (each sum accumulated onto a float bias, kAccBias, so that it reads back
+// as a float without a conversion); every float operation of the epilogues is written with
+// explicit round-to-nearest intrinsics in upstream's order, so outputs are bit-identical to the
 // HLSL semantics (as restated by the CPU oracle).  Every wait is bounded and reports a
 // timeout through the error word.
 #include <cstdint>
@@ -79,13 +80,30 @@ __device__ __forceinline__ int q8(float f)
   f = fminf(fmaxf(f, -128.0f), 127.0f);
   return __float_as_int(__fadd_rn(f, 12582912.0f)) - 0x4B400000;
 }
-// The same rounded value k in [-128, 127] as the float bits 0x4B400000 + k, whose low byte is
-// k's two's-complement byte (0x4B400000 has 22 zero low bits): pack bytes without subtracting.
-__device__ __forceinline__ uint32_t q8_bits(float f)
+// ClampS8(round(f)), HLSL round = nearest, ties to even, in one conversion (round to nearest
+// even, saturate to [-128, 127]): rounding then saturating equals clamping then rounding, the
+// bounds being integers.  The byte is the low byte of the result.
+__device__ __forceinline__ uint32_t s8_rne_sat(float f)
 {
-  f = fminf(fmaxf(f, -128.0f), 127.0f);
-  return __float_as_uint(__fadd_rn(f, 12582912.0f));
+  uint32_t r;
+  asm("cvt.rni.sat.s8.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return r;
 }
+
+// The s32 accumulators of the int8 MMAs start from kAccBias (the bits of the float 1.5 * 2^23),
+// so an accumulated sum s with |s| < 2^22 reads back as the float 12582912 + s exactly: one
+// packed subtraction gives (float)s, with no integer-to-float conversion.  The int8 products
+// bound every sum here: |s| <= 96 x 128 x 128 < 2^21.
+constexpr uint32_t kAccBias = 0x4B400000u;
+__device__ __forceinline__ void tmem_st_bias16(uint32_t taddr)
+{
+  const uint32_t v = kAccBias;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(v));
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // Low bytes of four words -> one word (byte i from word i).
 __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
@@ -227,8 +245,8 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
     }
 #pragma unroll
     for (int c = 0; c < C1; c += 2) {
-      put_byte(w, 4 * C0 + c, q8(__fmul_rn(blend[c / 2].x, 128.0f)));
-      put_byte(w, 4 * C0 + c + 1, q8(__fmul_rn(blend[c / 2].y, 128.0f)));
+      put_byte(w, 4 * C0 + c, (int)s8_rne_sat(__fmul_rn(blend[c / 2].x, 128.0f)));
+      put_byte(w, 4 * C0 + c + 1, (int)s8_rne_sat(__fmul_rn(blend[c / 2].y, 128.0f)));
     }
   }
   // 12 triangle waves of the texel coordinate at this lod, then the normalised lod
@@ -260,16 +278,14 @@ __device__ __forceinline__ void st16(uint8_t* base, int r, int c0, int cols, uin
 }
 
 // 16 accumulator columns of this thread's row -> 16 requantised activations (4 words).  The
-// arithmetic of hg_hlsl and q8_bits, two columns at a time on packed fp32 pairs (each lane
-// rounds exactly as the scalar operation).
+// arithmetic of hg_hlsl and q8, two columns at a time on packed fp32 pairs (each lane rounds
+// exactly as the scalar operation); the accumulators hold kAccBias + sum (see kAccBias).
 //
 // kFast (for 1.6e-5 <= rcp <= 600) forms the same bytes with fewer select / compare steps:
 // hardgelu as mid(max(min(x, 1.5), -1.5)) + (x - min(x, 1.5)), where the remainder is exact
 // for |x| < 2^23 and mid(1.5) = 1.5, so the sum is x above 1.5 and mid below (equal to the
 // select form for every float with |x| < 2^23, checked exhaustively on the CPU); from 2^23 up
-// both forms give at least 2^23, which saturates to 127 at rcp >= 1.6e-5.  hardgelu is at
-// least -0.1875, so at rcp <= 600 the scaled value stays above -113 and the lower clamp never
-// binds.
+// both forms give at least 2^23, which saturates to 127 at rcp >= 1.6e-5.
 template <bool kFast>
 __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restrict__ scale, float rcp, uint32_t* out)
 {
@@ -278,34 +294,31 @@ __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restric
   ptx::ld_wait();
   const float2 third = make_float2(1.0f / 3.0f, 1.0f / 3.0f), m3 = make_float2(-3.0f, -3.0f);
   const float2 h15 = make_float2(1.5f, 1.5f), r2 = make_float2(rcp, rcp), m1 = make_float2(-1.0f, -1.0f);
-  const float2 magic = make_float2(12582912.0f, 12582912.0f);
+  const float2 unbias = make_float2(-12582912.0f, -12582912.0f);
   uint32_t b[16];
 #pragma unroll
   for (int j = 0; j < 16; j += 2) {
-    const float2 x = ptx::mul2(make_float2((float)__float_as_int(acc[j]), (float)__float_as_int(acc[j + 1])),
-                               *reinterpret_cast<const float2*>(scale + j));
-    float2 f;
+    // (float)sum exactly, then times the row scale: as the conversion and multiply did
+    const float2 x =
+        ptx::mul2(ptx::add2(make_float2(acc[j], acc[j + 1]), unbias), *reinterpret_cast<const float2*>(scale + j));
+    float2 hg;
     if constexpr (kFast) {
       const float2 hi = make_float2(fminf(x.x, 1.5f), fminf(x.y, 1.5f));
       const float2 c = make_float2(fmaxf(hi.x, -1.5f), fmaxf(hi.y, -1.5f));
       const float2 q = ptx::mul2(c, third);
       const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);
       const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
-      const float2 hg = ptx::add2(mid, ptx::fma2(hi, m1, x));
-      f = ptx::mul2(hg, r2);
-      f = make_float2(fminf(f.x, 127.0f), fminf(f.y, 127.0f));
+      hg = ptx::add2(mid, ptx::fma2(hi, m1, x));
     } else {
       const float2 c = make_float2(fmaxf(x.x, -1.5f), fmaxf(x.y, -1.5f));
-      const float2 q = ptx::mul2(c, third);                    // div3: RN(c * RN(1/3)),
+      const float2 q = ptx::mul2(c, third);                        // div3: RN(c * RN(1/3)),
       const float2 q1 = ptx::fma2(ptx::fma2(q, m3, c), third, q);  // corrected by the exact remainder
       const float2 mid = ptx::mul2(q1, ptx::add2(c, h15));
-      const float2 hg = make_float2(x.x < 1.5f ? mid.x : x.x, x.y < 1.5f ? mid.y : x.y);
-      f = ptx::mul2(hg, r2);
-      f = make_float2(fminf(fmaxf(f.x, -128.0f), 127.0f), fminf(fmaxf(f.y, -128.0f), 127.0f));
+      hg = make_float2(x.x < 1.5f ? mid.x : x.x, x.y < 1.5f ? mid.y : x.y);
     }
-    const float2 k = ptx::add2(f, magic);
-    b[j] = __float_as_uint(k.x);
-    b[j + 1] = __float_as_uint(k.y);
+    const float2 f = ptx::mul2(hg, r2);
+    b[j] = s8_rne_sat(f.x);
+    b[j + 1] = s8_rne_sat(f.y);
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) out[i] = pack4(b[4 * i], b[4 * i + 1], b[4 * i + 2], b[4 * i + 3]);
@@ -313,7 +326,7 @@ __device__ __forceinline__ void requant16(uint32_t taddr, const float* __restric
 
 // One hidden layer's 64 columns of this thread's row, requantised into the next operand tile.
 __device__ __forceinline__ void requant_row(uint32_t taddr, const float* __restrict__ scale, float rcp, bool fast,
-                                            uint8_t* X, int row)
+                                            uint8_t* X, int row, int next_cols)
 {
   if (fast) {
 #pragma unroll
@@ -330,6 +343,9 @@ __device__ __forceinline__ void requant_row(uint32_t taddr, const float* __restr
       st16(X, row, c, kHid, q[0], q[1], q[2], q[3]);
     }
   }
+  // the next layer accumulates into the same columns, from the bias
+  for (int c = 0; c < next_cols; c += 16) tmem_st_bias16(taddr + c);
+  tmem_st_wait();
 }
 
 template <class SH>
@@ -525,34 +541,38 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
 #pragma unroll
       for (int c = 0; c < Kp; c += 16) st16(X, row, c, Kp, w[c / 4], w[c / 4 + 1], w[c / 4 + 2], w[c / 4 + 3]);
     }
+    // layer 0 accumulates from the bias (the previous tile's outputs were read before the last barrier)
+#pragma unroll
+    for (int c = 0; c < kHid; c += 16) tmem_st_bias16(lwin + c);
+    tmem_st_wait();
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < Kp / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, k > 0);
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a0 -> A (over X)
-    requant_row(lwin, s0, rcp1, fast1, X, row);
+    requant_row(lwin, s0, rcp1, fast1, X, row, kHid);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < kHid / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, k > 0);
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a1 -> A
-    requant_row(lwin, s1, rcp2, fast2, X, row);
+    requant_row(lwin, s1, rcp2, fast2, X, row, kOutRows);
     handoff();
     if (issuer) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < kHid / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, k > 0);
+        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, 1);
       ptx::commit(bar);
     }
     if (!wait_mma()) break;
@@ -563,8 +583,8 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::ld_wait();
       if (valid) {
 #pragma unroll
-        for (int c = 0; c < kOutRows; c++)  // saturate
-          acc[c] = fminf(1.0f, fmaxf(0.0f, __fmul_rn((float)__float_as_int(acc[c]), so[c])));
+        for (int c = 0; c < kOutRows; c++)  // (float)sum * scale, saturated by the multiply
+          acc[c] = __saturatef(__fmul_rn(__fsub_rn(acc[c], 12582912.0f), so[c]));
         if (A.material) {
           store_material(A.out + i * 18, acc, C, A);
         } else {
