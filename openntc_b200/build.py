@@ -72,6 +72,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
+    keep = set(objs)
+    for old in BUILD.glob("*.o"):  # objects of earlier source versions
+        if old not in keep:
+            old.unlink()
     return LIB
 
 

@@ -983,6 +983,7 @@ int ontc_init(ontc_context* c, int32_t profile, void* stream)
     return ONTC_ALLOCATION_FAILURE;
   }
   cudaMemset(c->W.p, 0, c->nW * sizeof(float));
+  cudaMemset(c->dWpart.p, 0, c->nW * sizeof(float));  // the accumulated gradient row starts at zero
   cudaMemset(c->tc_error.p, 0, 4 * sizeof(int));
   const size_t dec = (size_t)kHidden * c->Fp + kHidden * kHidden + kOutPad * kHidden + kHidden * 4 + kHidden * 4 +
                      kOutPad * 4;  // libopenntc.cpp:381-387
@@ -1255,6 +1256,7 @@ void ontc_begin_training(ontc_context* c, int32_t quality, int32_t grids_per_bat
   if (!e) e = cudaMemcpy(c->W.p, tmp.data(), c->nW * sizeof(float), cudaMemcpyHostToDevice);
   if (!e) e = cudaMemset(c->Wm.p, 0, c->nW * sizeof(float));
   if (!e) e = cudaMemset(c->Wv.p, 0, c->nW * sizeof(float));
+  if (!e) e = cudaMemset(c->dWpart.p, 0, c->nW * sizeof(float));  // after a tile kernel that stopped early
   if (!e) e = c->losses.alloc((size_t)std::max(c->batch_count, 1));
   if (!e) e = cudaMemset(c->losses.p, 0, c->losses.n * sizeof(double));
   // a failed start (no step-loss buffer, a failed upload) leaves the context in TrainError: no
@@ -1532,12 +1534,14 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
       c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
       c->launches++;
+      // the tcgen05 tile kernels add every CTA's decoder gradient into row 0 of dWpart
+      const bool dw_acc = cls != ONTC_KCLASS_UNITS_FP32;
       if (deferred) {
         const FootRec& now = look ? cross : fr;
         if (look && !e) e = cudaEventRecord(c->ev_tile, c->stream);
         c->prof_begin();
         if (!e)
-          e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, c->loss_part.p, grid, c->losses.p,
+          e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
                                       false, c->stream);
         // footprint latents: p, m, v, g in and out (32 B each)
         c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)now.cells[0] * c->C0 + (double)now.cells[1] * c->C1), 0.0);
@@ -1546,14 +1550,14 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
           if (!e) e = cudaStreamWaitEvent(c->side, c->ev_tile, 0);
           c->prof_begin(c->side);
           if (!e)
-            e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, nullptr, 0, nullptr, true, c->side);
+            e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, false, nullptr, 0, nullptr, true, c->side);
           c->prof_end(ONTC_KCLASS_SIDE_UPDATE, 32.0 * ((double)rest.cells[0] * c->C0 + (double)rest.cells[1] * c->C1),
                       0.0, c->side);
           c->launches++;
         }
       } else {
         c->prof_begin();
-        if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, c->loss_part.p, grid, c->losses.p, c->stream);
+        if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p, c->stream);
         // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
         c->prof_end(ONTC_KCLASS_ADAM,
                     s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
@@ -1962,14 +1966,18 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
   int grid = std::min(units, c->sms);
   const Model M = c->model();
   TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
+  bool acc = false;  // the tcgen05 tile kernels accumulate into row 0 (zero before and after)
+  if (!e) e = cudaMemsetAsync(c->dWpart.p, 0, c->nW * sizeof(float), c->stream);
   if (!e) {
     if (c->precision == ONTC_PRECISION_BF16 || c->precision == ONTC_PRECISION_BF16X3) {
+      acc = true;
       const bool split = c->precision == ONTC_PRECISION_BF16X3;
       const int gpc = tc_groups_per_cta(split);
       grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
       e = launch_tc_units(M, c->aux_steps.p, 0, grid, to, c->tc_error.p, c->boxes[s.lod], split, c->stream);
       if (e == cudaErrorNotSupported) {
         cudaGetLastError();
+        acc = false;
         grid = std::min(units, c->sms);
         e = launch_simt_units(kTrain, M, c->aux_steps.p, 0, grid, to, c->stream);
       }
@@ -1978,18 +1986,20 @@ int ontc_debug_gradients(ontc_context* c, ontc_debug_step* d, double* loss)
     }
     c->launches++;
   }
-  std::vector<float> part((size_t)grid * c->nW);
+  const int rows = acc ? 1 : grid;
+  std::vector<float> part((size_t)rows * c->nW);
   std::vector<double> lp(grid);
   if (!e) e = cudaStreamSynchronize(c->stream);
   if (!e && tc_failed(c)) e = cudaErrorLaunchTimeout;
   if (!e) e = cudaMemcpy(part.data(), c->dWpart.p, part.size() * sizeof(float), cudaMemcpyDeviceToHost);
   if (!e) e = cudaMemcpy(lp.data(), c->loss_part.p, lp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (!e) e = cudaMemset(c->dWpart.p, 0, c->nW * sizeof(float));
   if (e) return ONTC_CUDA_FAILURE;
   c->last_dW.assign(c->nW, 0.0f);
   for (int w = 0; w < c->nW; w++) {
-    double acc = 0.0;
-    for (int i = 0; i < grid; i++) acc += part[(size_t)i * c->nW + w];
-    c->last_dW[w] = (float)acc;
+    double sum = 0.0;
+    for (int i = 0; i < rows; i++) sum += part[(size_t)i * c->nW + w];
+    c->last_dW[w] = (float)sum;
   }
   double l = 0.0;
   for (double v : lp) l += v;

@@ -91,7 +91,8 @@ cudaError_t launch_decoded_sq_err(const TexelMap& m, int64_t j0, int64_t n, cons
 cudaError_t launch_wait_check(uint32_t polls, int* d_out, cudaStream_t stream);
 
 struct TileOut {
-  float* dW_partial;     // [grid][nW] per-CTA decoder gradient partial sums (kTrain)
+  float* dW_partial;     // kTrain: [grid][nW] per-CTA decoder gradient partials (SIMT kernel); the
+                         // tcgen05 tile kernel instead adds every CTA's gradient into row 0
   double* loss_partial;  // [grid] per-CTA sum of squared residuals (kTrain, kEval)
   float* calib_max;      // [2] running max |a0|, |a1| as ordered ints (kCalib)
 };
@@ -125,9 +126,10 @@ int tc_groups_per_cta(bool split);
 int tc_box_capacity();
 int tc_max_grid();
 
-// ---- optimiser: decoder Adam (reducing `grid` partials) + dense latent Adam/clamp/zero
-// of the step's level, one launch.  Also reduces the loss partials into loss_out[step].
-cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, const float* dW_partial,
+// ---- optimiser: decoder Adam (reducing `grid` partials, or with dw_acc reading and zeroing the
+// one row a tcgen05 tile kernel accumulates into) + dense latent Adam/clamp/zero of the step's
+// level, one launch.  Also reduces the `grid` loss partials into loss_out[step].
+cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, float* dW_partial, bool dw_acc,
                              const double* loss_partial, int grid, double* loss_out, cudaStream_t stream);
 // deferred latent optimiser (see optim.cu): catch the step's footprint up to its level step,
 // apply the step's gradient to the footprint (plus the decoder Adam), sweep a whole level
@@ -138,7 +140,7 @@ cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx,
 // the step's gradient on the footprint F and, with `decoder` (main instance only), the decoder
 // Adam + loss reduction; one launch
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
-                                    bool decoder, const float* dW_partial, const double* loss_partial, int grid,
+                                    bool decoder, float* dW_partial, bool dw_acc, const double* loss_partial, int grid,
                                     double* loss_out, bool side, cudaStream_t stream);
 // the hist-ring entries of steps [k0, k1) that update latents, from their step records
 cudaError_t launch_hist_write(const Model& M, const StepRec* d_steps, int k0, int k1, cudaStream_t stream);

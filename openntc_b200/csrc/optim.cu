@@ -61,11 +61,13 @@ __device__ __forceinline__ void adam_latent4(float* __restrict__ P, float* __res
 
 constexpr int kDecWarps = 8;  // warps of a decoder CTA, each summing every 8th partial
 
-// Decoder Adam for 32 weights (CTA `blk` of the decoder part, 256 threads): the `grid`
-// per-CTA gradient partials of the tile kernel split over 8 warps and combined in a fixed
-// order (deterministic).  CTA 0 also reduces the loss partials into loss_out[step].
+// Decoder Adam for 32 weights (CTA `blk` of the decoder part, 256 threads).  The gradient is
+// either the `grid` per-CTA partials of a tile kernel, split over 8 warps and combined in a
+// fixed order, or (dw_acc) the one row the tcgen05 tile kernel's CTAs add into, which is read
+// and then zeroed for the next step.  CTA 0 also reduces the `grid` loss partials into
+// loss_out[step].
 __device__ __forceinline__ void decoder_block(const Model& M, const StepRec& s, int blk,
-                                              const float* __restrict__ dW_partial,
+                                              float* __restrict__ dW_partial, bool dw_acc,
                                               const double* __restrict__ loss_partial, int grid,
                                               double* __restrict__ loss_out)
 {
@@ -81,13 +83,17 @@ __device__ __forceinline__ void decoder_block(const Model& M, const StepRec& s, 
   // upstream updates all of W0, W1 and the first C rows of Wout (libopenntc.cpp:722-754)
   const int nupd = min(M.nW, wo_off(M.F) + M.C * kHidden);
   const int w = blk * 32 + lane;
+  const int rows = dw_acc ? 1 : grid;
   float g = 0.0f;
   if (w < nupd) {
 #pragma unroll 4
-    for (int i = wp; i < grid; i += kDecWarps) g += dW_partial[(size_t)i * M.nW + w];
+    for (int i = wp; i < rows; i += kDecWarps) g += dW_partial[(size_t)i * M.nW + w];
   }
   red[wp][lane] = g;
   __syncthreads();
+  // row 0 is zero whenever a tile kernel starts: the accumulating one adds into it, the others
+  // overwrite it; every warp has read it by now
+  if (wp == 0 && w < M.nW) dW_partial[w] = 0.0f;
   if (wp != 0 || w >= nupd) return;
   g = red[0][lane];
 #pragma unroll
@@ -259,12 +265,12 @@ __global__ void __launch_bounds__(256) sweep_kernel(Model M, int lvl, int fl, in
 template <int C0, int C1, bool kSide>
 __global__ void __launch_bounds__(kSide ? kSideThreads : 256)
     footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx, const __grid_constant__ FootRec F,
-                            const float* __restrict__ dW_partial, const double* __restrict__ loss_partial, int grid,
-                            double* __restrict__ loss_out, int n_dec)
+                            float* __restrict__ dW_partial, bool dw_acc, const double* __restrict__ loss_partial,
+                            int grid, double* __restrict__ loss_out, int n_dec)
 {
   const StepRec& s = steps[idx];
   if (!kSide && (int)blockIdx.x < n_dec) {
-    decoder_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
+    decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
     return;
   }
   const int lvl = s.level, j = s.gstep;
@@ -289,13 +295,13 @@ __global__ void hist_write_kernel(Model M, const StepRec* __restrict__ steps, in
 }
 
 __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* __restrict__ steps, int step_idx,
-                                                        const float* __restrict__ dW_partial,
+                                                        float* __restrict__ dW_partial, bool dw_acc,
                                                         const double* __restrict__ loss_partial, int grid,
                                                         double* __restrict__ loss_out, int n_dec_blocks)
 {
   const StepRec& s = steps[step_idx];
   if ((int)blockIdx.x < n_dec_blocks) {
-    decoder_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
+    decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
     return;
   }
   if (!s.grid_update) return;
@@ -393,7 +399,7 @@ cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx,
 }
 
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
-                                    bool decoder, const float* dW_partial, const double* loss_partial, int grid,
+                                    bool decoder, float* dW_partial, bool dw_acc, const double* loss_partial, int grid,
                                     double* loss_out, bool side, cudaStream_t stream)
 {
   // the decoder CTAs are 256 threads (decoder_block): a launch with them is the main instance
@@ -405,11 +411,11 @@ cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int 
     if (side) {                                                                                          \
       if (total <= 0) return cudaSuccess;                                                                \
       footprint_update_kernel<a, b, true><<<(total + kSideThreads - 1) / kSideThreads, kSideThreads, 0,    \
-                                            stream>>>(M, d_steps, step_idx, F, nullptr, nullptr, 0, nullptr, 0); \
+                                            stream>>>(M, d_steps, step_idx, F, nullptr, false, nullptr, 0, nullptr, 0); \
     } else {                                                                                             \
       const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                   \
       if (blocks == 0) return cudaSuccess;                                                               \
-      footprint_update_kernel<a, b, false><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, \
+      footprint_update_kernel<a, b, false><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, dw_acc, \
                                                                        loss_partial, grid, loss_out, n_dec); \
     }                                                                                                    \
     return cudaGetLastError();                                                                           \
@@ -451,7 +457,7 @@ bool deferred_supported(int c0, int c1)
   return false;
 }
 
-cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, const float* dW_partial,
+cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_idx, float* dW_partial, bool dw_acc,
                              const double* loss_partial, int grid, double* loss_out, cudaStream_t stream)
 {
   // Sized for the largest level so one launch shape serves every step; CTAs beyond the
@@ -462,8 +468,8 @@ cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_id
   long long quads = (n0 + n1) / 4;
   long long lat_blocks = (quads + 255) / 256;
   if (lat_blocks > (long long)sm_count() * 8) lat_blocks = (long long)sm_count() * 8;
-  adam_step_kernel<<<(unsigned)(n_dec + lat_blocks), 256, 0, stream>>>(M, d_steps, step_idx, dW_partial, loss_partial,
-                                                                        grid, loss_out, n_dec);
+  adam_step_kernel<<<(unsigned)(n_dec + lat_blocks), 256, 0, stream>>>(M, d_steps, step_idx, dW_partial, dw_acc,
+                                                                        loss_partial, grid, loss_out, n_dec);
   return cudaGetLastError();
 }
 

@@ -79,6 +79,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int c0,
       : "memory");
 }
 
+// Relaxed gpu-scope reduction of four consecutive floats into global memory (16-byte aligned).
+__device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d)
+{
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
 // Asynchronous global -> shared copies (completion tracked per thread in commit groups).
 __device__ __forceinline__ void cp_async16(void* dst_smem, const void* src)
 {

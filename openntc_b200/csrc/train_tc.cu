@@ -1051,7 +1051,10 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (tid == 0) out.loss_partial[blockIdx.x] = ls;
   ptx::fence_after_sync();
   if (*(volatile int*)&fail_s == 0) {
-    float* dst = out.dW_partial + (size_t)blockIdx.x * M.nW;
+    // every CTA adds its gradient into the one accumulated row (the optimiser reads and zeroes
+    // it); F and the column steps are multiples of 4, so the 4-float runs are 16-byte aligned
+    static_assert(F % 4 == 0, "4-float gradient runs");
+    float* dst = out.dW_partial;
     const int lane = tid & 31;
     const int h = quad * 16 + lane;  // M=64 accumulators: row = lane of the quadrant's first 16
     const uint32_t la = tbase + lane_off;
@@ -1060,22 +1063,24 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       ptx::ld8(la + kColW0 + c, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 8; j++)
-          if (c + j < F) dst[w0_off() + h * F + c + j] = v[j];
+        for (int j = 0; j < 8; j += 4)
+          if (c + j < F) ptx::red_add4(dst + w0_off() + h * F + c + j, v[j], v[j + 1], v[j + 2], v[j + 3]);
     }
     for (int c = part * 16; c < 64; c += 16 * kParts) {
       float v[16];  // dW1[i][h]: accumulator row i, columns h, 16 per step
       ptx::ld16(la + kColW1 + c, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 16; j++) dst[w1_off(F) + h * 64 + c + j] = v[j];
+        for (int j = 0; j < 16; j += 4)
+          ptx::red_add4(dst + w1_off(F) + h * 64 + c + j, v[j], v[j + 1], v[j + 2], v[j + 3]);
     }
     for (int c = part * 8; c < 16; c += 8 * kParts) {
-      float v[8];  // dWout^T[h][c] -> dWout[c][h]
+      float v[8];  // dWout^T[h][c] -> dWout[c][h]; output rows past C carry no gradient
       ptx::ld8(la + kColWo + c, v);
       ptx::ld_wait();
       if (lane < 16)
-        for (int j = 0; j < 8; j++) dst[wo_off(F) + (c + j) * 64 + h] = v[j];
+        for (int j = 0; j < 8; j++)
+          if (c + j < M.C) atomicAdd(dst + wo_off(F) + (c + j) * 64 + h, v[j]);
     }
   } else if (tid == 0) {
     atomicExch(err, 1);
