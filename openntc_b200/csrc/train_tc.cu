@@ -547,6 +547,61 @@ __device__ __noinline__ void scatter_direct(LevelArgs L, int x, int y, int half,
   }
 }
 
+// ---- separable latent-gradient scatter of a staged unit ------------------------------------
+// Where a latent cell spans two or more texels each way, the corner sums factor into a pass
+// along x (texel columns -> box columns, one sum per texel row) and a pass along y (texel rows
+// -> box rows).  Pass 1 writes the x sums into an intermediate in shared memory:
+//   g0: T0[ty][bx][sy][C0] = sum over corner sides sx of the texels (ty, tx) whose side-sx
+//       corner column is bx, of their corner (sx, sy) feature gradient;
+//   g1: T1[ty][bx][C1]     = sum over sx of wx(sx, tx) times their g1 feature gradient,
+// and pass 2 sums T over the texel rows of each box row (weights wy for g1).  The products
+// and sums are those of the per-texel scatter (ntc_kernel.cu:317-340) regrouped.
+// dxs: the unit's feature gradients [128 texels][ld]; item i of the pass-1 index space.
+template <int C0>
+__device__ __forceinline__ void sep_pass1_g0(const float* dxs, int ld, const CornerMasks& cm, int w0, float inv0, int i,
+                                             float* T0)
+{
+  constexpr int Q0 = C0 / 4;
+  const int q = i % Q0, r = i / Q0;  // r = (ty * w0 + bx) * 2 + sy
+  const int sy = r & 1, tyb = r >> 1;
+  const int ty = div_small(tyb, inv0), bx = tyb - ty * w0;
+  const float* base = dxs + (ty << 4) * ld + 2 * sy * C0 + 4 * q;
+  float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint32_t m = cm.xlo[0][bx]; m; m &= m - 1) {
+    const float4 v = *reinterpret_cast<const float4*>(base + (__ffs(m) - 1) * ld);
+    sum.x += v.x, sum.y += v.y, sum.z += v.z, sum.w += v.w;
+  }
+  for (uint32_t m = cm.xhi[0][bx]; m; m &= m - 1) {
+    const float4 v = *reinterpret_cast<const float4*>(base + (__ffs(m) - 1) * ld + C0);
+    sum.x += v.x, sum.y += v.y, sum.z += v.z, sum.w += v.w;
+  }
+  *reinterpret_cast<float4*>(T0 + r * C0 + 4 * q) = sum;
+}
+
+template <int C0, int C1>
+__device__ __forceinline__ void sep_pass1_g1(const float* dxs, int ld, const CornerMasks& cm, int w1, float inv1, int j,
+                                             float* T1)
+{
+  constexpr int Q1 = C1 / 2;
+  const int q = j % Q1, r = j / Q1;  // r = ty * w1 + bx
+  const int ty = div_small(r, inv1), bx = r - ty * w1;
+  const float* base = dxs + (ty << 4) * ld + 4 * C0 + 2 * q;
+  float2 sum = make_float2(0.f, 0.f);
+  for (uint32_t m = cm.xlo[1][bx]; m; m &= m - 1) {
+    const int tx = __ffs(m) - 1;
+    const float w = 1.0f - cm.fx[tx];
+    const float2 v = *reinterpret_cast<const float2*>(base + tx * ld);
+    sum.x += w * v.x, sum.y += w * v.y;
+  }
+  for (uint32_t m = cm.xhi[1][bx]; m; m &= m - 1) {
+    const int tx = __ffs(m) - 1;
+    const float w = cm.fx[tx];
+    const float2 v = *reinterpret_cast<const float2*>(base + tx * ld);
+    sum.x += w * v.x, sum.y += w * v.y;
+  }
+  *reinterpret_cast<float2*>(T1 + r * C1 + 2 * q) = sum;
+}
+
 // Loads the fp32 master weights into the canonical operand tiles (zero padding past F / C).
 template <class SH, class E>
 __device__ void load_weights(const Model& M, uint8_t* W0, uint8_t* W1, uint8_t* Wo)
@@ -971,30 +1026,59 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       float* g0p = L.g0;
       float* g1p = L.g1;
       if (staged) {
-        // owner-computes: a work item is one box cell and a group of its channels (4 of g0,
-        // 2 of g1); its thread sums every texel-corner contribution to them
+        // A work item is one box cell and a group of its channels (4 of g0, 2 of g1), whose
+        // thread sums every texel-corner contribution to them and adds the sum with one vector
+        // reduction.  Per grid, where a cell spans two or more texels each way, the sums go
+        // through the separable passes (the intermediate in this unit's staging buffer, which
+        // nothing reads after the gather and the next unit's loads do not target); elsewhere
+        // the item's thread walks the corner masks itself.
         constexpr int Q0 = C0 / 4, Q1 = C1 / 2;
-        const int nc0 = f0.w * f0.h;
-        const int ni0 = nc0 * Q0;
-        const int ni = ni0 + f1.w * f1.h * Q1;
-        const float inv0 = 1.0f / (float)f0.w, inv1 = 1.0f / (float)f1.w;
+        const int w0 = f0.w, w1 = f1.w;
+        const float inv0 = 1.0f / (float)w0, inv1 = 1.0f / (float)w1;
+        const int n0 = 8 * w0 * 2 * C0, n1 = 8 * w1 * C1;  // intermediate floats
+        const bool sep1 = s.mip_dim >= 2 * d1 && n1 <= kFootBuf;
+        const bool sep0 = s.mip_dim >= 2 * d0 && n0 + (sep1 ? n1 : 0) <= kFootBuf;
+        float* T0 = foot;
+        float* T1 = foot + (sep0 ? n0 : 0);
+        const int p0 = sep0 ? 8 * w0 * 2 * Q0 : 0;
+        const int np = p0 + (sep1 ? 8 * w1 * Q1 : 0);
+        if (np > 0) {
+          for (int i = gt; i < np; i += kGroupThreads) {
+            if (i < p0)
+              sep_pass1_g0<C0>(dxs, LD, cm, w0, inv0, i, T0);
+            else
+              sep_pass1_g1<C0, C1>(dxs, LD, cm, w1, inv1, i - p0, T1);
+          }
+          bar_group(g);
+        }
+        const int ni0 = w0 * f0.h * Q0;
+        const int ni = ni0 + w1 * f1.h * Q1;
         for (int i = gt; i < ni; i += kGroupThreads) {
           if (i < ni0) {
             const int cell = i / Q0, q = i - cell * Q0;
-            const int by = div_small(cell, inv0), bx = cell - by * f0.w;
+            const int by = div_small(cell, inv0), bx = cell - by * w0;
             float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (sep0) {
+              // T0[ty][bx][sy]: rows whose side-sy corner row is by
 #pragma unroll
-            for (int kk = 0; kk < 4; kk++) {
-              const uint32_t mx = (kk & 1) ? cm.xhi[0][bx] : cm.xlo[0][bx];
-              const uint32_t my = (kk & 2) ? cm.yhi[0][by] : cm.ylo[0][by];
-              for (uint32_t ym = my; ym; ym &= ym - 1) {
-                const float* srow = dxs + ((__ffs(ym) - 1) << 4) * LD + kk * C0 + 4 * q;
-                for (uint32_t xm = mx; xm; xm &= xm - 1) {
-                  const float4 v = *reinterpret_cast<const float4*>(srow + (__ffs(xm) - 1) * LD);
-                  sum.x += v.x;
-                  sum.y += v.y;
-                  sum.z += v.z;
-                  sum.w += v.w;
+              for (int sy = 0; sy < 2; sy++) {
+                const float* t = T0 + (bx * 2 + sy) * C0 + 4 * q;
+                for (uint32_t ym = sy ? cm.yhi[0][by] : cm.ylo[0][by]; ym; ym &= ym - 1) {
+                  const float4 v = *reinterpret_cast<const float4*>(t + (__ffs(ym) - 1) * (w0 * 2 * C0));
+                  sum.x += v.x, sum.y += v.y, sum.z += v.z, sum.w += v.w;
+                }
+              }
+            } else {
+#pragma unroll
+              for (int kk = 0; kk < 4; kk++) {
+                const uint32_t mx = (kk & 1) ? cm.xhi[0][bx] : cm.xlo[0][bx];
+                const uint32_t my = (kk & 2) ? cm.yhi[0][by] : cm.ylo[0][by];
+                for (uint32_t ym = my; ym; ym &= ym - 1) {
+                  const float* srow = dxs + ((__ffs(ym) - 1) << 4) * LD + kk * C0 + 4 * q;
+                  for (uint32_t xm = mx; xm; xm &= xm - 1) {
+                    const float4 v = *reinterpret_cast<const float4*>(srow + (__ffs(xm) - 1) * LD);
+                    sum.x += v.x, sum.y += v.y, sum.z += v.z, sum.w += v.w;
+                  }
                 }
               }
             }
@@ -1006,25 +1090,38 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
           } else {
             const int j = i - ni0;
             const int cell = j / Q1, q = j - cell * Q1;
-            const int by = div_small(cell, inv1), bx = cell - by * f1.w;
+            const int by = div_small(cell, inv1), bx = cell - by * w1;
             float2 sum = make_float2(0.f, 0.f);
+            if (sep1) {
+              // T1[ty][bx]: weighted by the rows' side-sy fractions
+              const float* t = T1 + bx * C1 + 2 * q;
 #pragma unroll
-            for (int kk = 0; kk < 4; kk++) {
-              const uint32_t mx = (kk & 1) ? cm.xhi[1][bx] : cm.xlo[1][bx];
-              const uint32_t my = (kk & 2) ? cm.yhi[1][by] : cm.ylo[1][by];
-              for (uint32_t ym = my; ym; ym &= ym - 1) {
-                const int ty = __ffs(ym) - 1;
-                const float fy = cm.fy[ty];
-                const float wy = (kk & 2) ? fy : (1.0f - fy);
-                const float* srow = dxs + (ty << 4) * LD + 4 * C0 + 2 * q;
-                for (uint32_t xm = mx; xm; xm &= xm - 1) {
-                  const int tx = __ffs(xm) - 1;
-                  const float fx = cm.fx[tx];
-                  // the bilinear weight exactly as gather_geometry forms it
-                  const float w = ((kk & 1) ? fx : (1.0f - fx)) * wy;
-                  const float2 v = *reinterpret_cast<const float2*>(srow + tx * LD);
-                  sum.x += w * v.x;
-                  sum.y += w * v.y;
+              for (int sy = 0; sy < 2; sy++) {
+                for (uint32_t ym = sy ? cm.yhi[1][by] : cm.ylo[1][by]; ym; ym &= ym - 1) {
+                  const int ty = __ffs(ym) - 1;
+                  const float wy = sy ? cm.fy[ty] : 1.0f - cm.fy[ty];
+                  const float2 v = *reinterpret_cast<const float2*>(t + ty * (w1 * C1));
+                  sum.x += wy * v.x, sum.y += wy * v.y;
+                }
+              }
+            } else {
+#pragma unroll
+              for (int kk = 0; kk < 4; kk++) {
+                const uint32_t mx = (kk & 1) ? cm.xhi[1][bx] : cm.xlo[1][bx];
+                const uint32_t my = (kk & 2) ? cm.yhi[1][by] : cm.ylo[1][by];
+                for (uint32_t ym = my; ym; ym &= ym - 1) {
+                  const int ty = __ffs(ym) - 1;
+                  const float fy = cm.fy[ty];
+                  const float wy = (kk & 2) ? fy : (1.0f - fy);
+                  const float* srow = dxs + (ty << 4) * LD + 4 * C0 + 2 * q;
+                  for (uint32_t xm = mx; xm; xm &= xm - 1) {
+                    const int tx = __ffs(xm) - 1;
+                    const float fx = cm.fx[tx];
+                    // the bilinear weight exactly as gather_geometry forms it
+                    const float w = ((kk & 1) ? fx : (1.0f - fx)) * wy;
+                    const float2 v = *reinterpret_cast<const float2*>(srow + tx * LD);
+                    sum.x += w * v.x, sum.y += w * v.y;
+                  }
                 }
               }
             }
@@ -1032,6 +1129,8 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
             if (sum.x != 0.0f || sum.y != 0.0f) atomicAdd(reinterpret_cast<float2*>(dst), sum);
           }
         }
+        // the intermediate's generic writes before the staging buffer's next asynchronous load
+        if (np > 0) ptx::fence_proxy_async();
       } else if (valid) {
         scatter_direct<SH>(L, x, y, half, dxs + row * LD);
       }
