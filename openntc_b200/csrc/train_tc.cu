@@ -429,24 +429,42 @@ __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int r
     f++;
     if ((f & 7) == 0) st_chunk<E>(sX, row, col0 + f - 8, 128, Kp, buf);
   };
+  // vector loads: a cell's C0 (a multiple of 4) / C1 (even) floats start 16 / 8-byte aligned
   if (half == 0) {
+    float4 q[4][C0 / 4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int c = 0; c < C0; c += 4) q[k][c / 4] = *reinterpret_cast<const float4*>(L.p0 + G.c0[k] * C0 + c);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const int base = G.c0[k] * C0;
 #pragma unroll
-      for (int c = 0; c < C0; c++) put(L.p0[base + c] + level_noise(L, 0u, (uint32_t)(base + c)));
+      for (int c = 0; c < C0; c += 4) {
+        put(q[k][c / 4].x + level_noise(L, 0u, (uint32_t)(base + c)));
+        put(q[k][c / 4].y + level_noise(L, 0u, (uint32_t)(base + c + 1)));
+        put(q[k][c / 4].z + level_noise(L, 0u, (uint32_t)(base + c + 2)));
+        put(q[k][c / 4].w + level_noise(L, 0u, (uint32_t)(base + c + 3)));
+      }
     }
     return;
   }
   float acc[C1];
 #pragma unroll
   for (int c = 0; c < C1; c++) acc[c] = 0.0f;
+  float2 q[4][C1 / 2];
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int c = 0; c < C1; c += 2) q[k][c / 2] = *reinterpret_cast<const float2*>(L.p1 + G.c1[k] * C1 + c);
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     const int base = G.c1[k] * C1;
 #pragma unroll
-    for (int c = 0; c < C1; c++)
-      acc[c] = __fmaf_rn(G.w1[k], L.p1[base + c] + level_noise(L, 1u, (uint32_t)(base + c)), acc[c]);
+    for (int c = 0; c < C1; c += 2) {
+      acc[c] = __fmaf_rn(G.w1[k], q[k][c / 2].x + level_noise(L, 1u, (uint32_t)(base + c)), acc[c]);
+      acc[c + 1] = __fmaf_rn(G.w1[k], q[k][c / 2].y + level_noise(L, 1u, (uint32_t)(base + c + 1)), acc[c + 1]);
+    }
   }
 #pragma unroll
   for (int c = 0; c < C1; c++) put(acc[c]);
@@ -534,16 +552,26 @@ __device__ __noinline__ void scatter_direct(LevelArgs L, int x, int y, int half,
   constexpr int C0 = SH::C0, C1 = SH::C1;
   Gather G;
   gather_geometry(x, y, L.mip_dim, L.d0, L.d1, G);
+  // vector reductions (cells 16 / 8-byte aligned as in the gather); a group of exact zeros
+  // (a corner of zero bilinear weight) is left out: adding +0 changes no gradient
   if (half == 0) {
 #pragma unroll
     for (int kk = 0; kk < 4; kk++)
 #pragma unroll
-      for (int c = 0; c < C0; c++) atomicAdd(&L.g0[G.c0[kk] * C0 + c], dxr[kk * C0 + c]);
+      for (int c = 0; c < C0; c += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(dxr + kk * C0 + c);
+        if (v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f)
+          atomicAdd(reinterpret_cast<float4*>(L.g0 + G.c0[kk] * C0 + c), v);
+      }
   } else {
 #pragma unroll
     for (int kk = 0; kk < 4; kk++)
 #pragma unroll
-      for (int c = 0; c < C1; c++) atomicAdd(&L.g1[G.c1[kk] * C1 + c], G.w1[kk] * dxr[4 * C0 + c]);
+      for (int c = 0; c < C1; c += 2) {
+        const float2 d = *reinterpret_cast<const float2*>(dxr + 4 * C0 + c);
+        const float2 v = make_float2(G.w1[kk] * d.x, G.w1[kk] * d.y);
+        if (v.x != 0.0f || v.y != 0.0f) atomicAdd(reinterpret_cast<float2*>(L.g1 + G.c1[kk] * C1 + c), v);
+      }
   }
 }
 
