@@ -774,6 +774,9 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
   load_weights<SH, E>(M, sW0, sW1, sWo);
   if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
+  // corner masks start zeroed (each unit zeroes its own after its scatter)
+  static_assert(sizeof(CornerMasks) % 4 == 0, "mask words");
+  for (int i = tid; i < (int)(sizeof(masks_s) / 4); i += kThreads) reinterpret_cast<uint32_t*>(masks_s)[i] = 0u;
   static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
   if (tid < (int)(sizeof(StepRec) / 4))
     reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(steps + step_idx)[tid];
@@ -850,13 +853,26 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   bool nstaged = false;
   int pb = 0;
   uint32_t tph = 0, inflight = 0;
+  // buffer `buf`'s boxes landed (bounded wait; a timeout is reported, the buffer stays in
+  // flight and is waited for again before exit) and, with noise, perturbed in place
+  auto land = [&](int buf, const Foot& a0, const Foot& a1) {
+    if (ptx::mbar_wait(&tma_bars[g][buf], (tph >> buf) & 1u)) {
+      tph ^= 1u << buf;
+      inflight &= ~(1u << buf);
+    } else {
+      atomicExch(&fail_s, 1);
+    }
+    if (s.noise) stage_noise<SH>(L, boxes, a0, a1, gp.foot + buf * kFootBuf, gt);
+  };
   {
     const int u0 = blockIdx.x * E::kGroups + g;
     nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
     if (nstaged) {
       if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
       inflight |= 1u;
+      land(0, nf0, nf1);
     }
+    bar_group(g);  // the first unit's boxes before its gather
   }
 
   for (int unit = blockIdx.x * E::kGroups + g; unit < ntiles; unit += ustride) {
@@ -865,8 +881,24 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     const bool valid = b < s.texels;
     int x = 0, y = 0;
     if (valid) texel_xy(s, b, x, y);
-    // this thread's target channels [8 half, 8 half + 8): the loads are issued now and their
-    // values first used after layer 2, so their latency hides behind the forward pass
+    // this unit's boxes landed (and took their noise) during the previous unit, or in the
+    // prologue; its corner masks are built during its first MMAs
+    const Foot f0 = nf0, f1 = nf1;
+    const bool staged = nstaged;
+    const int cur = pb;
+    float* foot = gp.foot + cur * kFootBuf;
+    CornerMasks& cm = masks_s[g];
+    gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
+    handoff();
+    if (issuer) {
+      ptx::fence_after_sync();
+#pragma unroll
+      for (int k = 0; k < Kp / kK; k++) mma<E>(win, dXk, k * 256, kLoX, dW0k, k * 256, kLoW0, I_M128_N64_K, k > 0);
+      ptx::commit(bar);
+    }
+    // in the shadow of the MMAs: this thread's target channels [8 half, 8 half + 8) (first
+    // used after layer 2), and the next unit's box loads into the other staging buffer (its
+    // last readers, the previous unit's gather and scatter, finished before this unit began)
     uint32_t tb[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) tb[j] = 0u;
@@ -876,13 +908,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       for (int j = 0; j < 8; j++)
         if (half * 8 + j < C) tb[j] = tp[half * 8 + j];
     }
-    const Foot f0 = nf0, f1 = nf1;
-    const bool staged = nstaged;
-    const int cur = pb;
-    float* foot = gp.foot + cur * kFootBuf;
     {
-      // start the next unit's loads into the other buffer (its last reader, the gather of
-      // the unit before this one, finished several group barriers ago)
       const int nu = unit + ustride;
       nstaged = nu < ntiles && unit_footprint<SH>(L, s, boxes, nu, nf0, nf1);
       if (nstaged) {
@@ -890,34 +916,6 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         inflight |= 2u >> cur;
       }
       pb ^= 1;
-    }
-    CornerMasks& cm = masks_s[g];
-    if (staged) {
-      // this unit's boxes (bounded wait; a timeout is reported and the unit's results discarded)
-      if (ptx::mbar_wait(&tma_bars[g][cur], (tph >> cur) & 1u)) {
-        tph ^= 1u << cur;
-        inflight &= ~(1u << cur);
-      } else {
-        atomicExch(&fail_s, 1);  // still in flight: waited for again before exit
-      }
-      if (s.noise) stage_noise<SH>(L, boxes, f0, f1, foot, gt);
-      for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) {
-        uint32_t* m = i < 2 * kMaxBoxW ? &cm.xlo[0][0] + i
-                      : i < 4 * kMaxBoxW ? &cm.xhi[0][0] + (i - 2 * kMaxBoxW)
-                      : i < 4 * kMaxBoxW + 2 * kMaxBoxH ? &cm.ylo[0][0] + (i - 4 * kMaxBoxW)
-                                                       : &cm.yhi[0][0] + (i - 4 * kMaxBoxW - 2 * kMaxBoxH);
-        *m = 0u;
-      }
-      bar_group(g);
-      build_masks(s, L.d0, L.d1, f0, f1, unit, cm, gt);
-    }
-    gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
-    handoff();
-    if (issuer) {
-      ptx::fence_after_sync();
-#pragma unroll
-      for (int k = 0; k < Kp / kK; k++) mma<E>(win, dXk, k * 256, kLoX, dW0k, k * 256, kLoW0, I_M128_N64_K, k > 0);
-      ptx::commit(bar);
     }
     if (!wait_mma()) break;
 
@@ -936,6 +934,9 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       for (int k = 0; k < 64 / kK; k++) mma<E>(win, dP0k, k * 256, kLoP, dW1k, k * 256, kLoW1, I_M128_N64_K, k > 0);
       ptx::commit(bar);
     }
+    // this unit's corner masks (zeroed at the end of the previous unit), by the group's second
+    // warp while the first polls the MMA barrier
+    if (staged && (gt >> 5) == 1) build_masks(s, L.d0, L.d1, f0, f1, unit, cm, gt - 32);
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ layer 1 epilogue
@@ -1006,6 +1007,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
         mma<E>(tbase + kColW1, dP1m, k * kKS * S64, kLoP, dP0m, k * kKS * S64, kLoP, I_M64_N64_MN, 1);
       ptx::commit(bar);
     }
+    if (nstaged) land(cur ^ 1, nf0, nf1);  // the next unit's boxes, read after several barriers
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ dH0 (into P0)
@@ -1162,6 +1164,11 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
       } else if (valid) {
         scatter_direct<SH>(L, x, y, half, dxs + row * LD);
       }
+    }
+    if (staged) {
+      if (s.grid_update) bar_group(g);  // every read of the masks done
+      uint32_t* m = &cm.xlo[0][0];      // xlo, xhi, ylo, yhi: contiguous words
+      for (int i = gt; i < 2 * (2 * kMaxBoxW + 2 * kMaxBoxH); i += kGroupThreads) m[i] = 0u;
     }
     ptx::fence_before_sync();
     bar_group(g);
