@@ -62,6 +62,13 @@ int ontc_debug_last_step(ontc_context* ctx, ontc_debug_step* out);
  * Writes the mean squared residual to *loss.  Parameters are not updated. */
 int ontc_debug_gradients(ontc_context* ctx, ontc_debug_step* step, double* loss);
 
+/* The tile autotuner's cost of one unit round of the bf16 tcgen05 tile kernel at each lod, in
+ * microseconds (out_us[0 .. n), n >= the mip count): timed trials on scratch gradient buffers
+ * the first time (the training state is not touched), then the context's or the cache file's
+ * values.  ontc_train_batch splits the SMs of its shared tile launches by these costs.  No
+ * upstream counterpart. */
+int ontc_debug_tile_costs(ontc_context* ctx, float* out_us, int32_t n);
+
 /* Upstream quantize_pack on host floats through libontc's kernel (n * bits % 32 == 0). */
 int ontc_debug_quantize_pack(const float* host_in, int64_t n, int32_t bits, uint32_t* host_out);
 

@@ -152,6 +152,7 @@ SIGNATURES = {
     "ontc_debug_tensor": (C.c_int64, [P, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),
     "ontc_debug_last_step": (C.c_int, [P, C.POINTER(DebugStep)]),
     "ontc_debug_gradients": (C.c_int, [P, C.POINTER(DebugStep), C.POINTER(C.c_double)]),
+    "ontc_debug_tile_costs": (C.c_int, [P, C.POINTER(C.c_float), C.c_int32]),
     "ontc_debug_quantize_pack": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
     "ontc_debug_lanczos_down": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
     "ontc_debug_lanczos_weights": (C.c_int, [C.c_void_p]),

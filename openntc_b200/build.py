@@ -65,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if verbose and r.stderr.strip():
             sys.stderr.write(r.stderr)
     link = [str(NVCC)] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + [
-        "-L", str(CUDA / "lib64"), "-lcudart", "-lz"]
+        "-L", str(CUDA / "lib64"), "-lcudart", "-lz", "-Xlinker", "--no-undefined"]
     if verbose:
         print(" ".join(link), flush=True)
     r = subprocess.run(link, capture_output=True, text=True)

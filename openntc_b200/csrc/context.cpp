@@ -15,10 +15,12 @@
 // on one stream, the step's draws uploaded in batches ahead of time, no host sync per step,
 // quantisation noise generated at the touched latents only, FP64 loss and PSNR sums.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <bit>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iterator>
@@ -28,6 +30,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include "../../include/ontc.h"
 #include "../../include/ontc_debug.h"
@@ -235,6 +238,9 @@ struct ontc_context {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_pre = nullptr, ev_tile = nullptr, ev_cu = nullptr, ev_side = nullptr;
   bool side_pending = false;
+  // tile autotuner (shared batch launches): cost of one unit round of the tcgen05 tile kernel
+  // per lod, in microseconds; 0 until tuned
+  float unit_us[ONTC_MAX_MIPS] = {};
   DBuf<uint8_t> package[ONTC_MAX_MIPS];
   DBuf<uint32_t> packbuf;
   LatentBoxes boxes[ONTC_MAX_MIPS] = {};  // the tile kernel's TMA staging per lod
@@ -1342,8 +1348,9 @@ cudaError_t drain_side(ontc_context* c)
   return e;
 }
 
-// Draws and enqueues the next chunk of steps (at most 1024, ending at the lock step).
-//
+// Steps a chunk draws and enqueues at most (one slot each in the step records).
+constexpr int kChunkCap = 1024;
+
 // Per latent-updating step k of the deferred optimiser, when step k + 1 updates latents too
 // and needs no level sweep first (footprints F(k), F(k+1)):
 //   main: [catch-up of F(k) outside F(k-1): done on side] -> tile(k) -> decoder Adam + update
@@ -1355,32 +1362,55 @@ cudaError_t drain_side(ontc_context* c)
 // a cell of F(k+1) \ F(k) was last updated on side or before tile(k)), so the values are those
 // of the serial schedule bit for bit.  Otherwise step k runs serially on the main stream after
 // the side stream drains.
-cudaError_t enqueue_chunk(ontc_context* c, int target)
-{
-  std::bernoulli_distribution dist_batch_type(0.05);
-  std::uniform_real_distribution<float> dist_u(0.0f, 1.0f);
-  std::uniform_int_distribution<int> dist_lod(0, c->mips - 1);
-  const Model M = c->model();
-  const int chunk_cap = 1024;
-  // The previous chunk's kernels may still read the staging and device records.
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  if (e) return e;
-  const int first = c->batch_i;
-  int cnt = std::min(chunk_cap, target - first);
-  // a chunk ends at the lock step so the latents can be snapped before it runs
-  if (first < c->lock_i && first + cnt > c->lock_i) cnt = c->lock_i - first;
-  if ((int)c->foot_in.size() < chunk_cap) c->foot_in.resize(chunk_cap);
-  const bool deferred_mode = c->optimizer == ONTC_LATENT_ADAM_DEFERRED;
-  if (deferred_mode && !e) e = ensure_side(c);
+// One chunk of steps of one context, enqueued step by step: begin(), then per batch of up to
+// kPrepBatch steps prep(), and per step pre() (everything before the step's tile launch),
+// tile() (the context's own launch) and post() (everything after), then end().  enqueue_chunk
+// runs it alone; ontc_train_batch runs several in lock step around shared tile launches.
+struct ChunkRun {
+  static constexpr int kPrepBatch = 8;
+  ontc_context* c = nullptr;
+  std::bernoulli_distribution dist_batch_type{0.05};
+  std::uniform_real_distribution<float> dist_u{0.0f, 1.0f};
+  std::uniform_int_distribution<int> dist_lod;
+  Model M{};
+  int first = 0, cnt = 0;
+  int drawn = 0, uploaded = 0;
+  int ahead_step = -1;  // the step whose catch-up was enqueued on side
+  bool deferred_mode = false;
+  cudaError_t e = cudaSuccess;
+  // the step between pre() and post()
+  FootRec cross{}, rest{}, next_cu{};
+  bool look = false, deferred = false;
+  int grid = 0, cls = ONTC_KCLASS_UNITS_FP32;
+  int pre_k = -1;  // the last step pre() began
+
+  // Waits for the context's previous chunk and sizes this one: at most `cap` steps toward
+  // `target`, ending at the lock step.
+  cudaError_t begin(ontc_context* ctx, int target, int cap)
+  {
+    c = ctx;
+    dist_lod = std::uniform_int_distribution<int>(0, c->mips - 1);
+    M = c->model();
+    // The previous chunk's kernels may still read the staging and device records.
+    e = cudaStreamSynchronize(c->stream);
+    if (e) return e;
+    first = c->batch_i;
+    cnt = std::min(cap, target - first);
+    // a chunk ends at the lock step so the latents can be snapped before it runs
+    if (first < c->lock_i && first + cnt > c->lock_i) cnt = c->lock_i - first;
+    if ((int)c->foot_in.size() < kChunkCap) c->foot_in.resize(kChunkCap);
+    deferred_mode = c->optimizer == ONTC_LATENT_ADAM_DEFERRED;
+    if (deferred_mode && !e) e = ensure_side(c);
+    return e;
+  }
 
   // Steps are drawn in order, one ahead of the batch being launched (a step's lookahead needs
   // the next footprint), uploaded and launched kPrepBatch at a time, so the GPU starts after
   // the first few and the host prepares the rest while it runs (every step has its own slot).
-  constexpr int kPrepBatch = 8;
-  int drawn = 0, uploaded = 0;
-  int ahead_step = -1;  // the step whose catch-up was enqueued on side
-  for (int k0 = 0; k0 < cnt && e == cudaSuccess; k0 += kPrepBatch) {
-    const int k1 = std::min(cnt, k0 + kPrepBatch);
+  void prep(int k0, int k1)
+  {
+    (void)k0;
+    if (e) return;
     for (int k = drawn; k < std::min(cnt, k1 + 1); k++) {
       const int bi = first + k;
       const bool draw_uniform = dist_batch_type(c->gen);
@@ -1450,129 +1480,165 @@ cudaError_t enqueue_chunk(ontc_context* c, int target)
       c->launches++;
     }
     uploaded = drawn;
-    for (int k = k0; k < k1 && e == cudaSuccess; k++) {
-      const int bi = first + k;
-      const StepRec& s = c->h_steps[k];
-      const bool ahead = ahead_step == k;
-      if (!ahead) e = drain_side(c);
-      if (!e && c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
-        // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
-        for (int g = 0; g < 2 && e == cudaSuccess; g++)
-          e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
-                                g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
+  }
+
+  void pre(int k)
+  {
+    if (e) return;
+    pre_k = k;
+    const int bi = first + k;
+    const StepRec& s = c->h_steps[k];
+    const bool ahead = ahead_step == k;
+    if (!ahead) e = drain_side(c);
+    if (!e && c->noise_mode == ONTC_NOISE_UPSTREAM && bi < c->lock_i) {
+      // upstream regenerates the step level's noise buffers before every step (libopenntc.cpp:586-600)
+      for (int g = 0; g < 2 && e == cudaSuccess; g++)
+        e = launch_noise_fill(c->noise_states.p, ontc_context::kNoiseStates, (long long)c->level_elems(g, s.level),
+                              g == 0 ? c->d0 : c->d1, c->noise_buf[g].p, c->stream);
+      c->launches += 2;
+    }
+    if (!e && bi == c->lock_i) {
+      // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
+      if (deferred_mode) e = sweep_levels(c, c->lock_from, c->lock_to);
+      for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
+        e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
+        if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
         c->launches += 2;
       }
-      if (!e && bi == c->lock_i) {
-        // one-time snap of every level to its integer lattice (libopenntc.cpp:601-619)
-        if (deferred_mode) e = sweep_levels(c, c->lock_from, c->lock_to);
-        for (int l = 0; l < c->levels && e == cudaSuccess; l++) {
-          e = launch_quantize_grid(c->lat[0][0][l].p, (long long)c->level_elems(0, l), c->b0, c->d0, c->stream);
-          if (!e) e = launch_quantize_grid(c->lat[1][0][l].p, (long long)c->level_elems(1, l), c->b1, c->d1, c->stream);
-          c->launches += 2;
-        }
-        for (int g = 0; g < 2 && e == cudaSuccess; g++)
-          if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
-      }
-      const bool deferred = deferred_mode && s.grid_update;
-      const FootRec& fr = c->h_foots[k];
-      if (deferred && !ahead) {
-        if (s.sweep_from >= 0) {
-          c->prof_begin();
-          if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
-          c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)),
-                      0.0);
-          c->launches++;
-        }
+      for (int g = 0; g < 2 && e == cudaSuccess; g++)
+        if (c->noise_buf[g].p) e = cudaMemsetAsync(c->noise_buf[g].p, 0, c->noise_buf[g].n * sizeof(float), c->stream);
+    }
+    deferred = deferred_mode && s.grid_update;
+    const FootRec& fr = c->h_foots[k];
+    if (deferred && !ahead) {
+      if (s.sweep_from >= 0) {
         c->prof_begin();
-        if (!e) e = launch_catchup(M, c->steps.p, k, fr, false, c->stream);
-        // reads and writes p, m, v of the footprint latents that lag
-        c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
-        c->launches++;
-      }
-      if (ahead && !e) e = cudaStreamWaitEvent(c->stream, c->ev_cu, 0);
-      // the next step's catch-up outside this footprint, on side beside this tile kernel
-      FootRec cross, rest, next_cu;
-      bool look = false;
-      if (deferred && k + 1 < drawn) {
-        const StepRec& n = c->h_steps[k + 1];
-        look = n.grid_update && n.sweep_from < 0 &&
-               split_feet(s, fr, c->foot_in[k], n, c->h_foots[k + 1], c->foot_in[k + 1], cross, rest, next_cu);
-      }
-      if (look && !e) {
-        e = cudaEventRecord(c->ev_pre, c->stream);  // after the record uploads and this step's catch-up
-        if (!e) e = cudaStreamWaitEvent(c->side, c->ev_pre, 0);
-        c->prof_begin(c->side);
-        if (!e) e = launch_catchup(M, c->steps.p, k + 1, next_cu, true, c->side);
-        c->prof_end(ONTC_KCLASS_SIDE_CATCHUP,
-                    24.0 * ((double)next_cu.cells[0] * c->C0 + (double)next_cu.cells[1] * c->C1), 0.0, c->side);
-        c->launches++;
-        if (!e) e = cudaEventRecord(c->ev_cu, c->side);
-        ahead_step = k + 1;
-        c->side_pending = true;
-      }
-      const int units = (s.texels + kTile - 1) / kTile;
-      TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
-      int grid = std::min(units, c->sms);
-      int cls = ONTC_KCLASS_UNITS_FP32;
-      c->prof_begin();
-      if (e) {
-      } else if (c->precision == ONTC_PRECISION_BF16 || c->precision == ONTC_PRECISION_BF16X3) {
-        const bool split = c->precision == ONTC_PRECISION_BF16X3;
-        const int gpc = tc_groups_per_cta(split);  // work units in flight per CTA
-        grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
-        cls = split ? ONTC_KCLASS_UNITS_BF16X3 : ONTC_KCLASS_UNITS_BF16;
-        e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->boxes[s.lod], split, c->stream);
-        if (e == cudaErrorNotSupported) {
-          cudaGetLastError();
-          grid = std::min(units, c->sms);
-          cls = ONTC_KCLASS_UNITS_FP32;
-          e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
-        }
-      } else {
-        e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
-      }
-      // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
-      c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
-      c->launches++;
-      // the tcgen05 tile kernels add every CTA's decoder gradient into row 0 of dWpart
-      const bool dw_acc = cls != ONTC_KCLASS_UNITS_FP32;
-      if (deferred) {
-        const FootRec& now = look ? cross : fr;
-        if (look && !e) e = cudaEventRecord(c->ev_tile, c->stream);
-        c->prof_begin();
-        if (!e)
-          e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
-                                      false, c->stream);
-        // footprint latents: p, m, v, g in and out (32 B each)
-        c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)now.cells[0] * c->C0 + (double)now.cells[1] * c->C1), 0.0);
-        c->launches++;
-        if (look) {
-          if (!e) e = cudaStreamWaitEvent(c->side, c->ev_tile, 0);
-          c->prof_begin(c->side);
-          if (!e)
-            e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, false, nullptr, 0, nullptr, true, c->side);
-          c->prof_end(ONTC_KCLASS_SIDE_UPDATE, 32.0 * ((double)rest.cells[0] * c->C0 + (double)rest.cells[1] * c->C1),
-                      0.0, c->side);
-          c->launches++;
-        }
-      } else {
-        c->prof_begin();
-        if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p, c->stream);
-        // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
-        c->prof_end(ONTC_KCLASS_ADAM,
-                    s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
+        if (!e) e = launch_sweep(M, s.level, s.sweep_from, s.gstep, c->stream);
+        c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)),
                     0.0);
         c->launches++;
       }
-      c->last_seed = s.seed;
-      c->last_noise = s.noise != 0;
-      c->last_step = s;
-      c->texels_trained += s.texels;
-      c->batch_i = bi + 1;
+      c->prof_begin();
+      if (!e) e = launch_catchup(M, c->steps.p, k, fr, false, c->stream);
+      // reads and writes p, m, v of the footprint latents that lag
+      c->prof_end(ONTC_KCLASS_CATCHUP, 24.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
+      c->launches++;
+    }
+    if (ahead && !e) e = cudaStreamWaitEvent(c->stream, c->ev_cu, 0);
+    // the next step's catch-up outside this footprint, on side beside this tile kernel
+    look = false;
+    if (deferred && k + 1 < drawn) {
+      const StepRec& n = c->h_steps[k + 1];
+      look = n.grid_update && n.sweep_from < 0 &&
+             split_feet(s, fr, c->foot_in[k], n, c->h_foots[k + 1], c->foot_in[k + 1], cross, rest, next_cu);
+    }
+    if (look && !e) {
+      e = cudaEventRecord(c->ev_pre, c->stream);  // after the record uploads and this step's catch-up
+      if (!e) e = cudaStreamWaitEvent(c->side, c->ev_pre, 0);
+      c->prof_begin(c->side);
+      if (!e) e = launch_catchup(M, c->steps.p, k + 1, next_cu, true, c->side);
+      c->prof_end(ONTC_KCLASS_SIDE_CATCHUP,
+                  24.0 * ((double)next_cu.cells[0] * c->C0 + (double)next_cu.cells[1] * c->C1), 0.0, c->side);
+      c->launches++;
+      if (!e) e = cudaEventRecord(c->ev_cu, c->side);
+      ahead_step = k + 1;
+      c->side_pending = true;
     }
   }
-  const cudaError_t d = drain_side(c);
-  return e ? e : d;
+
+  void tile(int k)
+  {
+    const StepRec& s = c->h_steps[k];
+    const int units = (s.texels + kTile - 1) / kTile;
+    TileOut to = {c->dWpart.p, c->loss_part.p, nullptr};
+    grid = std::min(units, c->sms);
+    cls = ONTC_KCLASS_UNITS_FP32;
+    c->prof_begin();
+    if (e) {
+    } else if (c->precision == ONTC_PRECISION_BF16 || c->precision == ONTC_PRECISION_BF16X3) {
+      const bool split = c->precision == ONTC_PRECISION_BF16X3;
+      const int gpc = tc_groups_per_cta(split);  // work units in flight per CTA
+      grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
+      cls = split ? ONTC_KCLASS_UNITS_BF16X3 : ONTC_KCLASS_UNITS_BF16;
+      e = launch_tc_units(M, c->steps.p, k, grid, to, c->tc_error.p, c->boxes[s.lod], split, c->stream);
+      if (e == cudaErrorNotSupported) {
+        cudaGetLastError();
+        grid = std::min(units, c->sms);
+        cls = ONTC_KCLASS_UNITS_FP32;
+        e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+      }
+    } else {
+      e = launch_simt_units(kTrain, M, c->steps.p, k, grid, to, c->stream);
+    }
+    // MLP fwd + both backward GEMMs per texel: 3 x 2 x (64 F + 64*64 + 64 C) flops
+    c->prof_end(cls, (double)s.texels * c->C, 6.0 * (double)s.texels * (64.0 * c->F + 4096.0 + 64.0 * c->C));
+    c->launches++;
+  }
+
+  void post(int k)
+  {
+    const int bi = first + k;
+    const StepRec& s = c->h_steps[k];
+    const FootRec& fr = c->h_foots[k];
+    // the tcgen05 tile kernels add every CTA's decoder gradient into row 0 of dWpart
+    const bool dw_acc = cls != ONTC_KCLASS_UNITS_FP32;
+    if (deferred) {
+      const FootRec& now = look ? cross : fr;
+      if (look && !e) e = cudaEventRecord(c->ev_tile, c->stream);
+      c->prof_begin();
+      if (!e)
+        e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
+                                    false, c->stream);
+      // footprint latents: p, m, v, g in and out (32 B each)
+      c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)now.cells[0] * c->C0 + (double)now.cells[1] * c->C1), 0.0);
+      c->launches++;
+      if (look) {
+        if (!e) e = cudaStreamWaitEvent(c->side, c->ev_tile, 0);
+        c->prof_begin(c->side);
+        if (!e)
+          e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, false, nullptr, 0, nullptr, true, c->side);
+        c->prof_end(ONTC_KCLASS_SIDE_UPDATE, 32.0 * ((double)rest.cells[0] * c->C0 + (double)rest.cells[1] * c->C1),
+                    0.0, c->side);
+        c->launches++;
+      }
+    } else {
+      c->prof_begin();
+      if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p, c->stream);
+      // latent Adam streams p, m, v, g in and out once: 32 bytes per latent of the level
+      c->prof_end(ONTC_KCLASS_ADAM,
+                  s.grid_update ? 32.0 * (double)(c->level_elems(0, s.level) + c->level_elems(1, s.level)) : 0.0,
+                  0.0);
+      c->launches++;
+    }
+    c->last_seed = s.seed;
+    c->last_noise = s.noise != 0;
+    c->last_step = s;
+    c->texels_trained += s.texels;
+    c->batch_i = bi + 1;
+  }
+
+  cudaError_t end()
+  {
+    const cudaError_t d = drain_side(c);
+    return e ? e : d;
+  }
+};
+
+// Draws and enqueues the next chunk of steps (at most kChunkCap, ending at the lock step).
+cudaError_t enqueue_chunk(ontc_context* c, int target)
+{
+  ChunkRun r;
+  if (r.begin(c, target, kChunkCap)) return r.e;
+  for (int k0 = 0; k0 < r.cnt && r.e == cudaSuccess; k0 += ChunkRun::kPrepBatch) {
+    const int k1 = std::min(r.cnt, k0 + ChunkRun::kPrepBatch);
+    r.prep(k0, k1);
+    for (int k = k0; k < k1 && r.e == cudaSuccess; k++) {
+      r.pre(k);
+      r.tile(k);
+      r.post(k);
+    }
+  }
+  return r.end();
 }
 
 // Ends a run of ontc_train chunks: every latent current, the stream drained and checked, the
@@ -1629,6 +1695,321 @@ void ontc_train(ontc_context* c, int32_t num_batches, ontc_train_progress* out)
 
 void ontc_train_until_complete(ontc_context* c, ontc_train_progress* out) { ontc_train(c, c->batch_count, out); }
 
+}  // extern "C"
+
+namespace {
+
+// Steps the next chunk of context c toward `target` holds (as ChunkRun::begin sizes it).
+int chunk_steps(const ontc_context* c, int target)
+{
+  int cnt = std::min(kChunkCap, target - c->batch_i);
+  if (c->batch_i < c->lock_i && c->batch_i + cnt > c->lock_i) cnt = c->lock_i - c->batch_i;
+  return cnt;
+}
+
+// CTAs of a shared tile launch per material: one each, then every further SM to the material
+// that takes longest (its unit rounds, units / (gpc x CTAs) rounded up, times its measured
+// cost of a round), as long as one still gains from it; the launch lasts as long as its
+// longest material.
+void partition_ctas(const std::vector<int>& units, const std::vector<float>& cost, int gpc, int sms,
+                    std::vector<int>& ctas)
+{
+  const int n = (int)units.size();
+  ctas.assign(n, 1);
+  auto time = [&](int i) { return (float)((units[i] + gpc * ctas[i] - 1) / (gpc * ctas[i])) * cost[i]; };
+  for (int used = n; used < sms; used++) {
+    int best = -1;
+    for (int i = 0; i < n; i++) {
+      if (ctas[i] * gpc >= units[i]) continue;  // one unit per group already
+      if (best < 0 || time(i) > time(best) || (time(i) == time(best) && units[i] > units[best])) best = i;
+    }
+    if (best < 0) break;
+    ctas[best]++;
+  }
+}
+
+// ---- tile autotuner -------------------------------------------------------------------------
+// The cost of one unit round (each group of every CTA through one 128-texel unit) of a
+// context's tcgen05 tile kernel, per lod: it depends on the profile shape and on how the lod's
+// texels fall on the latent grids (staged boxes or not, separable scatter or not).  Measured by
+// timed trial launches of a representative step on scratch gradient buffers (the training
+// state is not touched), kept in the context and in a cache file: ONTC_TUNE_CACHE, else
+// $XDG_CACHE_HOME or ~/.cache + /openntc_b200/tile_costs.txt (ONTC_TUNE_CACHE="" keeps them in
+// memory only).  Lines: "<device>|<C0>,<C1>,<Fp>|<mip>,<d0>,<d1>,<texels> <microseconds>".
+std::string tune_cache_path()
+{
+  if (const char* p = getenv("ONTC_TUNE_CACHE")) return p;
+  std::string base;
+  if (const char* x = getenv("XDG_CACHE_HOME"); x && *x) base = x;
+  else if (const char* h = getenv("HOME"); h && *h) base = std::string(h) + "/.cache";
+  else return "";
+  return base + "/openntc_b200/tile_costs.txt";
+}
+
+std::string tune_key(const ontc_context* c, int lod, const char* device)
+{
+  const int level = c->feature_level_for_lod(lod), mip = c->mip_dim[lod];
+  const int tile = std::min(mip, 256);
+  char k[256];
+  snprintf(k, sizeof(k), "%s|%d,%d,%d|%d,%d,%d,%d", device, c->C0, c->C1, c->model().Fp, mip, c->g0_dim[level],
+           c->g1_dim[level], c->grids * tile * tile);
+  for (char* q = k; *q; q++)
+    if (*q == ' ') *q = '_';
+  return k;
+}
+
+cudaError_t tune_tiles(ontc_context* c)
+{
+  bool done = true;
+  for (int l = 0; l < c->mips; l++) done = done && c->unit_us[l] > 0.0f;
+  if (done) return cudaSuccess;
+  int dev = 0;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (!e) e = cudaGetDeviceProperties(&prop, dev);
+  if (e) return e;
+  // cached costs
+  const std::string path = tune_cache_path();
+  std::vector<std::pair<std::string, float>> cached;
+  if (!path.empty()) {
+    std::ifstream f(path);
+    std::string key;
+    float us;
+    while (f >> key >> us) cached.emplace_back(key, us);
+  }
+  std::vector<int> todo;
+  for (int l = 0; l < c->mips; l++) {
+    if (c->unit_us[l] > 0.0f) continue;
+    const std::string key = tune_key(c, l, prop.name);
+    for (const auto& kv : cached)
+      if (kv.first == key) c->unit_us[l] = kv.second;
+    if (c->unit_us[l] <= 0.0f) todo.push_back(l);
+  }
+  if (todo.empty()) return cudaSuccess;
+  // trials on scratch gradients, losses and error flag
+  size_t g0n = 0, g1n = 0;
+  for (int l = 0; l < c->levels; l++) {
+    g0n = std::max(g0n, c->level_elems(0, l));
+    g1n = std::max(g1n, c->level_elems(1, l));
+  }
+  DBuf<float> g0s, g1s, dws;
+  DBuf<double> lps;
+  DBuf<int> errs;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  e = cudaStreamSynchronize(c->stream);
+  if (!e) e = g0s.alloc(g0n);
+  if (!e) e = g1s.alloc(g1n);
+  if (!e) e = dws.alloc(c->nW);
+  if (!e) e = lps.alloc(c->max_grid);
+  if (!e) e = errs.alloc(4);
+  if (!e) e = cudaMemsetAsync(errs.p, 0, 4 * sizeof(int), c->stream);
+  if (!e) e = cudaEventCreate(&t0);
+  if (!e) e = cudaEventCreate(&t1);
+  std::vector<StepRec> recs(c->mips);
+  for (int l = 0; l < c->mips && !e; l++) {
+    StepRec& s = recs[l];
+    s = StepRec();
+    s.lod = l;
+    s.level = c->feature_level_for_lod(l);
+    s.mip_dim = c->mip_dim[l];
+    s.tile_dim = std::min(s.mip_dim, 256);
+    s.n_grids = c->grids;
+    s.texels = c->grids * s.tile_dim * s.tile_dim;
+    s.noise = 1;
+    s.grid_update = 1;
+    s.seed = 12345u + (uint32_t)l;
+    s.norm_lod = l / static_cast<float>(c->mips - 1);
+    for (int g = 0; g < c->grids; g++) {  // spread over the mip, as the uniform draws are
+      s.ox[g] = (int)(((int64_t)(2 * g + 1) * s.mip_dim * 37) / 101) % s.mip_dim;
+      s.oy[g] = (int)(((int64_t)(2 * g + 1) * s.mip_dim * 59) / 103) % s.mip_dim;
+    }
+  }
+  if (!e) e = cudaMemcpyAsync(c->aux_steps.p, recs.data(), c->mips * sizeof(StepRec), cudaMemcpyHostToDevice, c->stream);
+  std::vector<std::string> lines;
+  for (int l : todo) {
+    if (e) break;
+    const StepRec& s = recs[l];
+    Model M = c->model();
+    M.g0.g[s.level] = g0s.p;
+    M.g1.g[s.level] = g1s.p;
+    const TileOut to = {dws.p, lps.p, nullptr};
+    const int units = (s.texels + kTile - 1) / kTile, gpc = tc_groups_per_cta(false);
+    const int grid = std::min((units + gpc - 1) / gpc, tc_max_grid());
+    float best = 0.0f;
+    for (int rep = 0; rep < 4 && !e; rep++) {  // one warm-up, then the fastest of three
+      e = cudaEventRecord(t0, c->stream);
+      if (!e) e = launch_tc_units(M, c->aux_steps.p, l, grid, to, errs.p, c->boxes[l], false, c->stream);
+      if (!e) e = cudaEventRecord(t1, c->stream);
+      if (!e) e = cudaEventSynchronize(t1);
+      float ms = 0.0f;
+      if (!e) e = cudaEventElapsedTime(&ms, t0, t1);
+      c->launches++;
+      if (rep > 0 && (best == 0.0f || ms < best)) best = ms;
+    }
+    if (e) break;
+    const int rounds = (units + gpc * grid - 1) / (gpc * grid);
+    c->unit_us[l] = std::max(1e-3f, 1e3f * best / (float)rounds);
+    char v[32];
+    snprintf(v, sizeof(v), " %.4f", c->unit_us[l]);
+    lines.push_back(tune_key(c, l, prop.name) + v);
+  }
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  int flag[4] = {};
+  if (!e) e = cudaMemcpy(flag, errs.p, sizeof(flag), cudaMemcpyDeviceToHost);
+  if (!e && flag[0]) e = cudaErrorLaunchTimeout;  // a bounded wait gave up: no costs from it
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  if (e) {
+    for (int l : todo) c->unit_us[l] = 0.0f;
+    return e;
+  }
+  if (!path.empty() && !lines.empty()) {
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos) {
+      std::string dir = path.substr(0, slash);
+      for (size_t i = 1; i <= dir.size(); i++)  // mkdir -p
+        if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+    }
+    std::ofstream f(path, std::ios::app);
+    for (const auto& line : lines) f << line << "\n";
+  }
+  return cudaSuccess;
+}
+
+// The streams and events of shared tile launches: a stream per profile shape, an event per
+// context (its step's work before the tile) and per shape (the shared tile done).
+struct SharedTiles {
+  std::vector<cudaStream_t> stream;
+  std::vector<cudaEvent_t> ev_tile, ev_pre;
+  ~SharedTiles()
+  {
+    for (cudaStream_t st : stream)
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
+    for (cudaEvent_t ev : ev_tile) if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ev_pre) if (ev) cudaEventDestroy(ev);
+  }
+  cudaError_t init(int n_ctx, int n_shapes)
+  {
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    stream.assign(n_shapes, nullptr);
+    ev_tile.assign(n_shapes, nullptr);
+    ev_pre.assign(n_ctx, nullptr);
+    for (auto& st : stream) if (!e) e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, greatest);
+    for (auto& ev : ev_tile) if (!e) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    for (auto& ev : ev_pre) if (!e) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    return e;
+  }
+};
+
+// Step k of every context in `live` (runs[i] between pre(k) and post(k)) in one tcgen05 tile
+// launch per profile shape: the SMs are shared among all the materials, each material's CTAs
+// run its own step.  Sets each run's grid and kernel class for its post(k).
+void shared_tile_step(ontc_context* const* ctxs, std::vector<ChunkRun>& runs, const std::vector<int>& live,
+                      const std::vector<int>& shape_of, SharedTiles& st, int k)
+{
+  std::vector<int> in, units, ctas;
+  for (int i : live)
+    if (runs[i].e == cudaSuccess) {
+      in.push_back(i);
+      units.push_back((ctxs[i]->h_steps[k].texels + kTile - 1) / kTile);
+    }
+  if (in.empty()) return;
+  std::vector<float> cost;
+  for (int i : in) {
+    const float us = ctxs[i]->unit_us[ctxs[i]->h_steps[k].lod];
+    cost.push_back(us > 0.0f ? us : 1.0f);
+  }
+  partition_ctas(units, cost, tc_groups_per_cta(false), tc_max_grid(), ctas);
+  for (int sh = 0; sh < (int)st.stream.size(); sh++) {
+    TileMat mats[kMaxTileMats];
+    int idx[kMaxTileMats];
+    int nm = 0, begin = 0;
+    for (int j = 0; j < (int)in.size(); j++) {
+      const int i = in[j];
+      if (shape_of[i] != sh) continue;
+      ontc_context* c = ctxs[i];
+      const StepRec& s = c->h_steps[k];
+      TileMat& t = mats[nm];
+      memset(&t, 0, sizeof(t));
+      t.boxes = c->boxes[s.lod];
+      t.M = runs[i].M;
+      t.step = c->steps.p + k;
+      t.out = TileOut{c->dWpart.p, c->loss_part.p, nullptr};
+      t.err = c->tc_error.p;
+      t.cta_begin = begin;
+      t.cta_count = ctas[j];
+      begin += ctas[j];
+      idx[nm++] = i;
+    }
+    if (nm == 0) continue;
+    cudaError_t e = cudaSuccess;
+    for (int m = 0; m < nm && !e; m++) {
+      e = cudaEventRecord(st.ev_pre[idx[m]], ctxs[idx[m]]->stream);
+      if (!e) e = cudaStreamWaitEvent(st.stream[sh], st.ev_pre[idx[m]], 0);
+    }
+    if (!e) e = launch_tc_multi(mats, nm, st.stream[sh]);
+    if (!e) e = cudaEventRecord(st.ev_tile[sh], st.stream[sh]);
+    ctxs[idx[0]]->launches++;
+    for (int m = 0; m < nm; m++) {
+      ChunkRun& r = runs[idx[m]];
+      if (!e) e = cudaStreamWaitEvent(ctxs[idx[m]]->stream, st.ev_tile[sh], 0);
+      r.grid = mats[m].cta_count;
+      r.cls = ONTC_KCLASS_UNITS_BF16;
+    }
+    if (e)
+      for (int m = 0; m < nm; m++) runs[idx[m]].e = e;
+  }
+}
+
+// The contexts of ontc_train_batch advanced in lock step, chunk by chunk, with shared tile
+// launches.  err[i] receives each context's outcome.
+void train_shared(ontc_context* const* ctxs, const std::vector<int>& target, const std::vector<char>& active,
+                  const std::vector<int>& shape_of, int n_shapes, std::vector<cudaError_t>& err)
+{
+  const int n = (int)target.size();
+  SharedTiles st;
+  const cudaError_t se = st.init(n, n_shapes);
+  // unit-round costs per lod for the SM split (timed once, cached); without them every unit
+  // round counts the same
+  for (int i = 0; i < n; i++)
+    if (active[i] && err[i] == cudaSuccess && !se && tune_tiles(ctxs[i]) != cudaSuccess) cudaGetLastError();
+  std::vector<ChunkRun> runs(n);
+  for (;;) {
+    std::vector<int> live;
+    for (int i = 0; i < n; i++)
+      if (active[i] && err[i] == cudaSuccess && ctxs[i]->batch_i < target[i]) {
+        if (se) err[i] = se;
+        else live.push_back(i);
+      }
+    if (live.empty()) return;
+    int cap = kChunkCap;
+    for (int i : live) cap = std::min(cap, chunk_steps(ctxs[i], target[i]));
+    for (int i : live) {
+      runs[i] = ChunkRun();
+      runs[i].begin(ctxs[i], target[i], cap);
+    }
+    for (int k0 = 0; k0 < cap; k0 += ChunkRun::kPrepBatch) {
+      const int k1 = std::min(cap, k0 + ChunkRun::kPrepBatch);
+      for (int i : live) runs[i].prep(k0, k1);
+      for (int k = k0; k < k1; k++) {
+        for (int i : live) runs[i].pre(k);
+        shared_tile_step(ctxs, runs, live, shape_of, st, k);
+        for (int i : live)
+          if (runs[i].pre_k == k) runs[i].post(k);
+      }
+    }
+    for (int i : live) err[i] = runs[i].end();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
 int ontc_train_batch(ontc_context* const* ctxs, int32_t n, int32_t num_batches, ontc_train_progress* out)
 {
   if (n < 0 || (n > 0 && (!ctxs || !out))) return ONTC_INVALID_STATE;
@@ -1657,9 +2038,34 @@ int ontc_train_batch(ontc_context* const* ctxs, int32_t n, int32_t num_batches, 
     }
     active[i] = 1;
   }
-  // one chunk per context in turn: while the host waits for one context's previous chunk,
-  // the others' kernels run on their own streams
-  for (bool more = true; more;) {
+  // BF16 contexts (at most kMaxTileMats of each profile shape) share their tile launches: one
+  // per shape and step, its SMs split among the materials
+  std::vector<int> shape_of(n, -1);
+  std::vector<std::array<int, 3>> shapes;
+  std::vector<int> per_shape;
+  bool shared = true;
+  int n_active = 0;
+  for (int i = 0; i < n; i++) {
+    if (!active[i]) continue;
+    n_active++;
+    const ontc_context* c = ctxs[i];
+    if (c->precision != ONTC_PRECISION_BF16) shared = false;
+    const std::array<int, 3> key = {c->C0, c->C1, c->model().Fp};
+    int sh = 0;
+    while (sh < (int)shapes.size() && shapes[sh] != key) sh++;
+    if (sh == (int)shapes.size()) {
+      shapes.push_back(key);
+      per_shape.push_back(0);
+    }
+    shape_of[i] = sh;
+    if (++per_shape[sh] > kMaxTileMats) shared = false;
+  }
+  if (shared && n_active >= 2) {
+    train_shared(ctxs, target, active, shape_of, (int)shapes.size(), err);
+  }
+  // otherwise one chunk per context in turn: while the host waits for one context's previous
+  // chunk, the others' kernels run on their own streams
+  for (bool more = !(shared && n_active >= 2); more;) {
     more = false;
     for (int i = 0; i < n; i++) {
       ontc_context* c = ctxs[i];
@@ -1934,6 +2340,14 @@ int ontc_debug_last_step(ontc_context* c, ontc_debug_step* o)
   o->gb1 = s.gb1;
   o->gb2 = s.gb2;
   o->grid_update = s.grid_update;
+  return ONTC_SUCCESS;
+}
+
+int ontc_debug_tile_costs(ontc_context* c, float* out_us, int32_t n)
+{
+  if (!c->manifest_loaded || !out_us || n < c->mips) return ONTC_INVALID_STATE;
+  if (tune_tiles(c) != cudaSuccess) return ONTC_CUDA_FAILURE;
+  for (int l = 0; l < n; l++) out_us[l] = l < c->mips ? c->unit_us[l] : 0.0f;
   return ONTC_SUCCESS;
 }
 

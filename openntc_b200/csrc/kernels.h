@@ -120,6 +120,20 @@ cudaError_t launch_simt_units(int mode, const Model& M, const StepRec* d_steps, 
 // cudaErrorNotSupported when the profile has no tcgen05 variant
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out,
                             int* d_error, const LatentBoxes& boxes, bool split, cudaStream_t stream);
+// Many materials in one tcgen05 tile launch (bf16 operands): material i runs its step on CTAs
+// [cta_begin, cta_begin + cta_count), which follow one another from 0 in material order; every
+// material has the same profile shape.  Each material's loss partials are indexed by its own
+// CTAs, and its decoder gradient is added into row 0 of its dW buffer as in launch_tc_units.
+constexpr int kMaxTileMats = 16;
+struct alignas(64) TileMat {
+  LatentBoxes boxes;   // the tensor maps of the step's lod (first: 64-byte aligned)
+  Model M;
+  const StepRec* step;  // the material's step record on the device
+  TileOut out;
+  int* err;             // the material's tile error flag
+  int32_t cta_begin, cta_count;
+};
+cudaError_t launch_tc_multi(const TileMat* mats, int n, cudaStream_t stream);
 // 128-texel units a tile CTA works on at once (its grid: units / this, at most one CTA per SM)
 int tc_groups_per_cta(bool split);
 // the staging buffer the tile kernel gives a unit's latent boxes, in floats

@@ -712,11 +712,28 @@ __device__ __forceinline__ void tmem_st_zero16(uint32_t taddr)
       "r"(z));
 }
 
-template <class SH, class E>
-__global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1)
-tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut out, int* __restrict__ err,
-               const __grid_constant__ LatentBoxes boxes)
+// One material's share of a tile launch: CTAs [cta_begin, cta_begin + cta_count) run its step.
+template <int kMats>
+struct TileJob {
+  TileMat mat[kMats];
+  int32_t n;
+};
+
+template <class SH, class E, int kMats>
+__global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(const __grid_constant__ TileJob<kMats> J)
 {
+  // this CTA's material (materials in CTA order) and its place among the material's CTAs
+  int mi = 0;
+  if constexpr (kMats > 1) {
+    for (int i = 1; i < J.n; i++)
+      if ((int)blockIdx.x >= J.mat[i].cta_begin) mi = i;
+  }
+  const TileMat& T = J.mat[mi];
+  const Model& M = T.M;
+  const LatentBoxes& boxes = T.boxes;
+  const TileOut& out = T.out;
+  int* __restrict__ err = T.err;
+  const int cta = (int)blockIdx.x - T.cta_begin, ncta = T.cta_count;
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp, F = SH::F;
   constexpr int kThreads = E::kGroups * kGroupThreads;
   constexpr int kParts = E::kGroups * 2;  // splits of the per-CTA epilogue work
@@ -779,7 +796,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   for (int i = tid; i < (int)(sizeof(masks_s) / 4); i += kThreads) reinterpret_cast<uint32_t*>(masks_s)[i] = 0u;
   static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
   if (tid < (int)(sizeof(StepRec) / 4))
-    reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(steps + step_idx)[tid];
+    reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(T.step)[tid];
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
@@ -848,7 +865,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   // latent boxes: unit k's were loaded (TMA, asynchronously) while unit k-1 ran, into the
   // staging buffer the previous unit did not use; tph holds each buffer's next wait parity and
   // inflight which buffers have loads not yet waited for
-  const int ustride = gridDim.x * E::kGroups;
+  const int ustride = ncta * E::kGroups;
   Foot nf0 = {}, nf1 = {};
   bool nstaged = false;
   int pb = 0;
@@ -865,7 +882,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     if (s.noise) stage_noise<SH>(L, boxes, a0, a1, gp.foot + buf * kFootBuf, gt);
   };
   {
-    const int u0 = blockIdx.x * E::kGroups + g;
+    const int u0 = cta * E::kGroups + g;
     nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
     if (nstaged) {
       if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
@@ -875,7 +892,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
     bar_group(g);  // the first unit's boxes before its gather
   }
 
-  for (int unit = blockIdx.x * E::kGroups + g; unit < ntiles; unit += ustride) {
+  for (int unit = cta * E::kGroups + g; unit < ntiles; unit += ustride) {
     // ------------------------------------------------------------------ gather
     const int b = unit * kTile + row;
     const bool valid = b < s.texels;
@@ -1182,7 +1199,7 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
 
   // ------------------------------------------------------------------ weight gradients out
   const double ls = block_sum_d_tc<kThreads>(loss, red);
-  if (tid == 0) out.loss_partial[blockIdx.x] = ls;
+  if (tid == 0) out.loss_partial[cta] = ls;
   ptx::fence_after_sync();
   if (*(volatile int*)&fail_s == 0) {
     // every CTA adds its gradient into the one accumulated row (the optimiser reads and zeroes
@@ -1224,31 +1241,25 @@ tc_unit_kernel(Model M, const StepRec* __restrict__ steps, int step_idx, TileOut
   if (warp == 0) ptx::tmem_dealloc(tbase, kTmemCols);
 }
 
-template <class SH, class E>
-cudaError_t launch_shape(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                         const LatentBoxes& boxes, cudaStream_t stream)
+template <class SH, class E, int kMats>
+cudaError_t launch_shape(const TileJob<kMats>& job, int grid, cudaStream_t stream)
 {
   constexpr size_t smem = smem_bytes<SH, E>();
   static_assert(smem <= 227 * 1024 - 6 * 1024, "shared memory budget (dynamic + static)");
-  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(tc_unit_kernel<SH, E, kMats>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tc_unit_kernel<SH, E><<<grid, E::kGroups * kGroupThreads, smem, stream>>>(M, d_steps, step_idx, out, d_error, boxes);
+  tc_unit_kernel<SH, E, kMats><<<grid, E::kGroups * kGroupThreads, smem, stream>>>(job);
   return cudaGetLastError();
 }
 
-template <class E>
-cudaError_t launch_elem(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
-                        const LatentBoxes& boxes, cudaStream_t stream)
+template <class E, int kMats>
+cudaError_t launch_elem(const Model& M, const TileJob<kMats>& job, int grid, cudaStream_t stream)
 {
   // profile shapes (libopenntc.cpp:289-333): C0, C1, padded feature dim
-  if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64)
-    return launch_shape<Shape<8, 12, 64>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96)
-    return launch_shape<Shape<12, 20, 96>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80)
-    return launch_shape<Shape<12, 10, 80>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
-  if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96)
-    return launch_shape<Shape<16, 12, 96>, E>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  if (M.C0 == 8 && M.C1 == 12 && M.Fp == 64) return launch_shape<Shape<8, 12, 64>, E>(job, grid, stream);
+  if (M.C0 == 12 && M.C1 == 20 && M.Fp == 96) return launch_shape<Shape<12, 20, 96>, E>(job, grid, stream);
+  if (M.C0 == 12 && M.C1 == 10 && M.Fp == 80) return launch_shape<Shape<12, 10, 80>, E>(job, grid, stream);
+  if (M.C0 == 16 && M.C1 == 12 && M.Fp == 96) return launch_shape<Shape<16, 12, 96>, E>(job, grid, stream);
   return cudaErrorNotSupported;
 }
 
@@ -1265,8 +1276,33 @@ int tc_max_grid()
 cudaError_t launch_tc_units(const Model& M, const StepRec* d_steps, int step_idx, int grid, TileOut out, int* d_error,
                             const LatentBoxes& boxes, bool split, cudaStream_t stream)
 {
-  return split ? launch_elem<ESplit>(M, d_steps, step_idx, grid, out, d_error, boxes, stream)
-              : launch_elem<EBf16>(M, d_steps, step_idx, grid, out, d_error, boxes, stream);
+  TileJob<1> job;
+  job.mat[0].boxes = boxes;
+  job.mat[0].M = M;
+  job.mat[0].step = d_steps + step_idx;
+  job.mat[0].out = out;
+  job.mat[0].err = d_error;
+  job.mat[0].cta_begin = 0;
+  job.mat[0].cta_count = grid;
+  job.n = 1;
+  return split ? launch_elem<ESplit, 1>(M, job, grid, stream) : launch_elem<EBf16, 1>(M, job, grid, stream);
+}
+
+cudaError_t launch_tc_multi(const TileMat* mats, int n, cudaStream_t stream)
+{
+  if (n < 1 || n > kMaxTileMats) return cudaErrorInvalidValue;
+  TileJob<kMaxTileMats> job;
+  memset(&job, 0, sizeof(job));
+  int grid = 0;
+  for (int i = 0; i < n; i++) {
+    const Model& a = mats[i].M;
+    if (a.C0 != mats[0].M.C0 || a.C1 != mats[0].M.C1 || a.Fp != mats[0].M.Fp) return cudaErrorInvalidValue;
+    if (mats[i].cta_begin != grid || mats[i].cta_count < 1) return cudaErrorInvalidValue;
+    job.mat[i] = mats[i];
+    grid += mats[i].cta_count;
+  }
+  job.n = n;
+  return launch_elem<EBf16, kMaxTileMats>(mats[0].M, job, grid, stream);
 }
 
 int tc_groups_per_cta(bool split) { return split ? ESplit::kGroups : EBf16::kGroups; }

@@ -52,3 +52,76 @@ def test_batch_rejects_a_context_twice_and_reports_finished_ones(materials):
     assert r == ont.Result.Success
     assert prog[0].phase == ont.TrainPhase.TrainComplete and prog[0].batches_complete == 30
     assert prog[1].phase == ont.TrainPhase.TrainInProgress and prog[1].batches_complete == 10
+
+
+# BF16 contexts share their tile launches: one tcgen05 launch per profile shape and step, the
+# SMs split among that step's materials (three Bpp_1_0 materials share one launch here)
+MIX_BF16 = [(256, 9, ont.Profile.Bpp_1_0), (512, 9, ont.Profile.Bpp_1_0), (256, 4, ont.Profile.Bpp_0_2),
+            (256, 12, ont.Profile.Bpp_2_25), (512, 6, ont.Profile.Bpp_1_0)]
+
+
+def _bf16_contexts(materials, steps):
+    return [H.new_context(p, materials(dim, 40 + i, ch), min_dim=16, grids=2, steps=steps,
+                          precision=ont.Precision.BF16)
+            for i, (dim, ch, p) in enumerate(MIX_BF16)]
+
+
+def test_bf16_batch_shares_tile_launches(materials):
+    """The shared launches train every material as its own ontc_train does, within the run-to-run
+    spread of the bf16 tile kernel (its decoder gradients are summed in arrival order): step
+    losses within 2 %, final PSNR within 0.05 dB.  The launch counts show the sharing: each
+    step's shared launch is counted once per shape, so the batch issues steps x (materials -
+    shapes) fewer launches than the separate runs."""
+    steps = 120
+    solo = _bf16_contexts(materials, steps)
+    solo_second = 0
+    for c in solo:  # the same calls as the batch below, so the same chunks and flushes
+        assert c.train(70).result == 0
+        before = c.kernel_launches()
+        assert c.train(1000).phase == ont.TrainPhase.TrainComplete
+        solo_second += c.kernel_launches() - before
+    batch = _bf16_contexts(materials, steps)
+    r, prog = ont.train_batch(batch, 70)  # also times the autotuner's trials
+    assert r == ont.Result.Success and [p.batches_complete for p in prog] == [70] * len(MIX_BF16)
+    before = sum(c.kernel_launches() for c in batch)
+    r, prog = ont.train_batch(batch, 1000)
+    assert r == ont.Result.Success
+    assert all(p.phase == ont.TrainPhase.TrainComplete and p.batches_complete == steps for p in prog)
+    shapes = len({p for _, _, p in MIX_BF16})
+    batch_second = sum(c.kernel_launches() for c in batch) - before
+    assert solo_second - batch_second == (steps - 70) * (len(MIX_BF16) - shapes)
+    for a, b in zip(solo, batch):
+        la, lb = np.array(a.step_losses(steps)), np.array(b.step_losses(steps))
+        assert np.all(np.isfinite(lb))
+        assert np.allclose(la, lb, rtol=2e-2, atol=0), np.abs(la / lb - 1).max()
+        assert abs(a.eval().psnr - b.eval().psnr) < 0.05
+
+
+def test_tile_autotuner_times_each_lod_once_and_caches(materials, tmp_path, monkeypatch):
+    """ontc_train_batch splits a shared launch's SMs by the measured cost of a unit round at
+    each material's lod: timed once per lod (one warm-up and three timed trial launches), then
+    read back from the cache file by any context of the same shape and sizes."""
+    import ctypes as C
+    cache = tmp_path / "tile_costs.txt"
+    monkeypatch.setenv("ONTC_TUNE_CACHE", str(cache))
+    manifest = materials(512, 50, 9)
+
+    def costs(ctx):
+        n = H.shape(ctx)["mips"]
+        buf = (C.c_float * n)()
+        before = ctx.kernel_launches()
+        assert ctx._lib.ontc_debug_tile_costs(ctx.handle, buf, n) == 0
+        return list(buf), ctx.kernel_launches() - before
+
+    a = H.new_context(ont.Profile.Bpp_1_0, manifest, min_dim=16, grids=2, steps=20, precision=ont.Precision.BF16)
+    first, launched = costs(a)
+    assert all(c > 0 for c in first) and launched == 4 * len(first)
+    assert len(cache.read_text().splitlines()) == len(first)
+    again, launched = costs(a)
+    assert again == first and launched == 0
+    b = H.new_context(ont.Profile.Bpp_1_0, manifest, min_dim=16, grids=2, steps=20, precision=ont.Precision.BF16)
+    cached, launched = costs(b)
+    assert launched == 0 and np.allclose(cached, first, rtol=1e-3, atol=1e-4)
+    # the trials leave the training state alone: training after them still completes and learns
+    p = a.train_until_complete()
+    assert p.phase == ont.TrainPhase.TrainComplete and np.isfinite(a.eval().psnr)
