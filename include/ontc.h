@@ -226,11 +226,14 @@ int ontc_set_train_options(ontc_context* ctx, const ontc_train_options* opts);
 void ontc_train(ontc_context* ctx, int32_t num_batches, ontc_train_progress* out);
 /* Context::TrainUntilComplete (libopenntc.cpp:529) */
 void ontc_train_until_complete(ontc_context* ctx, ontc_train_progress* out);
-/* No upstream counterpart (the batch entry point for many materials): advances each of the n
- * contexts by up to num_batches steps, exactly as n ontc_train calls would, but enqueues their
- * step chunks in turn so that the kernels of different contexts overlap on the GPU (give each
- * context its own stream).  out[i] receives context i's progress; returns ONTC_SUCCESS or the
- * first failing context's result.  A context may appear only once. */
+/* No upstream counterpart (the batch entry point for many materials; it generalises upstream's
+ * grids_per_batch_, libopenntc.h:162): advances each of the n contexts by up to num_batches
+ * steps as n ontc_train calls would.  BF16 contexts (at most 16 of each profile) run in lock
+ * step and share one tile-kernel launch per profile and step, its SMs split among them by
+ * per-lod costs that a first autotuning pass measures and caches (ontc_debug_tile_costs);
+ * otherwise the contexts' step chunks are enqueued in turn so that their kernels overlap on
+ * the GPU (give each context its own stream).  out[i] receives context i's progress; returns
+ * ONTC_SUCCESS or the first failing context's result.  A context may appear only once. */
 int ontc_train_batch(ontc_context* const* ctxs, int32_t n, int32_t num_batches, ontc_train_progress* out);
 
 /* Context::Eval (libopenntc.cpp:972).  FP64 reduction. */
