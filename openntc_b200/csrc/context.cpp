@@ -1354,14 +1354,13 @@ constexpr int kChunkCap = 1024;
 // Per latent-updating step k of the deferred optimiser, when step k + 1 updates latents too
 // and needs no level sweep first (footprints F(k), F(k+1)):
 //   main: [catch-up of F(k) outside F(k-1): done on side] -> tile(k) -> decoder Adam + update
-//         of F(k) n F(k+1) -> tile(k+1) ...
-//   side: catch-up of F(k+1) \ F(k), beside tile(k), after the step records are uploaded;
-//         then, after tile(k), the update of F(k) \ F(k+1), beside tile(k+1).
-// The side kernels touch no latent the concurrent tile kernel or main-stream update reads or
-// writes, and every cell's updates and replays keep their order (the side stream is in order;
-// a cell of F(k+1) \ F(k) was last updated on side or before tile(k)), so the values are those
-// of the serial schedule bit for bit.  Otherwise step k runs serially on the main stream after
-// the side stream drains.
+//         of F(k) -> tile(k+1) ...
+//   side: catch-up of F(k+1) \ F(k), after the step records are uploaded (it runs as SMs free
+//         up: beside the end of tile(k) and the update of F(k)).
+// The side kernel touches no latent the concurrent tile kernel or main-stream update reads or
+// writes, and every cell's updates and replays keep their order (a cell of F(k+1) \ F(k) was
+// last updated before tile(k)), so the values are those of the serial schedule bit for bit.
+// Otherwise step k runs serially on the main stream after the side stream drains.
 // One chunk of steps of one context, enqueued step by step: begin(), then per batch of up to
 // kPrepBatch steps prep(), and per step pre() (everything before the step's tile launch),
 // tile() (the context's own launch) and post() (everything after), then end().  enqueue_chunk
@@ -1586,24 +1585,16 @@ struct ChunkRun {
     // the tcgen05 tile kernels add every CTA's decoder gradient into row 0 of dWpart
     const bool dw_acc = cls != ONTC_KCLASS_UNITS_FP32;
     if (deferred) {
-      const FootRec& now = look ? cross : fr;
-      if (look && !e) e = cudaEventRecord(c->ev_tile, c->stream);
+      // the whole footprint on the main stream, beside the next step's catch-up on side (they
+      // touch disjoint cells); a tile CTA fills its SM's register file, so an update left for
+      // the side stream would only run between tile launches anyway
       c->prof_begin();
       if (!e)
-        e = launch_footprint_update(M, c->steps.p, k, now, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
+        e = launch_footprint_update(M, c->steps.p, k, fr, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
                                     false, c->stream);
       // footprint latents: p, m, v, g in and out (32 B each)
-      c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)now.cells[0] * c->C0 + (double)now.cells[1] * c->C1), 0.0);
+      c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
       c->launches++;
-      if (look) {
-        if (!e) e = cudaStreamWaitEvent(c->side, c->ev_tile, 0);
-        c->prof_begin(c->side);
-        if (!e)
-          e = launch_footprint_update(M, c->steps.p, k, rest, false, nullptr, false, nullptr, 0, nullptr, true, c->side);
-        c->prof_end(ONTC_KCLASS_SIDE_UPDATE, 32.0 * ((double)rest.cells[0] * c->C0 + (double)rest.cells[1] * c->C1),
-                    0.0, c->side);
-        c->launches++;
-      }
     } else {
       c->prof_begin();
       if (!e) e = launch_adam_step(M, c->steps.p, k, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p, c->stream);
