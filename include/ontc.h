@@ -381,7 +381,8 @@ enum {
   ONTC_KCLASS_ADAM = 2,       /* fused decoder + latent Adam / clamp / gradient-zero pass */
   ONTC_KCLASS_CATCHUP = 3,    /* deferred optimiser: footprint catch-up and level sweeps */
   ONTC_KCLASS_SIDE_CATCHUP = 4, /* the next step's catch-up, on the side stream beside a tile kernel */
-  ONTC_KCLASS_SIDE_UPDATE = 5,  /* a step's footprint update outside the next footprint, side stream */
+  ONTC_KCLASS_SIDE_UPDATE = 5,  /* kept for the numbering: the whole footprint update now runs in
+                                  ONTC_KCLASS_ADAM, so no launch falls in this class */
   ONTC_KCLASS_UNITS_BF16X3 = 6, /* the tile kernel, tcgen05 split-bf16 (BF16X3) */
   ONTC_KCLASS_COUNT = 7
 };

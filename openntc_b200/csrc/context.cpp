@@ -1591,7 +1591,7 @@ struct ChunkRun {
       c->prof_begin();
       if (!e)
         e = launch_footprint_update(M, c->steps.p, k, fr, true, c->dWpart.p, dw_acc, c->loss_part.p, grid, c->losses.p,
-                                    false, c->stream);
+                                    c->stream);
       // footprint latents: p, m, v, g in and out (32 B each)
       c->prof_end(ONTC_KCLASS_ADAM, 32.0 * ((double)fr.cells[0] * c->C0 + (double)fr.cells[1] * c->C1), 0.0);
       c->launches++;

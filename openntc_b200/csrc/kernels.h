@@ -151,11 +151,11 @@ cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_id
 // otherwise 256-thread CTAs
 cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F, bool side,
                            cudaStream_t stream);
-// the step's gradient on the footprint F and, with `decoder` (main instance only), the decoder
-// Adam + loss reduction; one launch
+// the step's gradient on the footprint F and, with `decoder`, the decoder Adam + loss
+// reduction; one launch
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
                                     bool decoder, float* dW_partial, bool dw_acc, const double* loss_partial, int grid,
-                                    double* loss_out, bool side, cudaStream_t stream);
+                                    double* loss_out, cudaStream_t stream);
 // the hist-ring entries of steps [k0, k1) that update latents, from their step records
 cudaError_t launch_hist_write(const Model& M, const StepRec* d_steps, int k0, int k1, cudaStream_t stream);
 // every latent of `level` from level step max(applied, from) to J

@@ -262,14 +262,14 @@ __global__ void __launch_bounds__(256) sweep_kernel(Model M, int lvl, int fl, in
 
 // Decoder Adam (CTAs [0, n_dec)) and the step's gradient on its footprint, every latent of
 // which is at level step gstep (the other CTAs).
-template <int C0, int C1, bool kSide>
-__global__ void __launch_bounds__(kSide ? kSideThreads : 256)
+template <int C0, int C1>
+__global__ void __launch_bounds__(256)
     footprint_update_kernel(Model M, const StepRec* __restrict__ steps, int idx, const __grid_constant__ FootRec F,
                             float* __restrict__ dW_partial, bool dw_acc, const double* __restrict__ loss_partial,
                             int grid, double* __restrict__ loss_out, int n_dec)
 {
   const StepRec& s = steps[idx];
-  if (!kSide && (int)blockIdx.x < n_dec) {
+  if ((int)blockIdx.x < n_dec) {
     decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
     return;
   }
@@ -400,24 +400,16 @@ cudaError_t launch_catchup(const Model& M, const StepRec* d_steps, int step_idx,
 
 cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int step_idx, const FootRec& F,
                                     bool decoder, float* dW_partial, bool dw_acc, const double* loss_partial, int grid,
-                                    double* loss_out, bool side, cudaStream_t stream)
+                                    double* loss_out, cudaStream_t stream)
 {
-  // the decoder CTAs are 256 threads (decoder_block): a launch with them is the main instance
-  if (decoder && side) return cudaErrorInvalidValue;
   const int n_dec = decoder ? dec_blocks(M) : 0;
 #define X(a, b)                                                                                          \
   if (M.g0.channels == a && M.g1.channels == b) {                                                        \
     const int total = F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q;                             \
-    if (side) {                                                                                          \
-      if (total <= 0) return cudaSuccess;                                                                \
-      footprint_update_kernel<a, b, true><<<(total + kSideThreads - 1) / kSideThreads, kSideThreads, 0,    \
-                                            stream>>>(M, d_steps, step_idx, F, nullptr, false, nullptr, 0, nullptr, 0); \
-    } else {                                                                                             \
-      const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                   \
-      if (blocks == 0) return cudaSuccess;                                                               \
-      footprint_update_kernel<a, b, false><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, dw_acc, \
-                                                                       loss_partial, grid, loss_out, n_dec); \
-    }                                                                                                    \
+    const unsigned blocks = (unsigned)(n_dec + (total + 255) / 256);                                     \
+    if (blocks == 0) return cudaSuccess;                                                                 \
+    footprint_update_kernel<a, b><<<blocks, 256, 0, stream>>>(M, d_steps, step_idx, F, dW_partial, dw_acc,   \
+                                                              loss_partial, grid, loss_out, n_dec);      \
     return cudaGetLastError();                                                                           \
   }
   ONTC_FOR_CHANNEL_PAIRS(X)
