@@ -13,6 +13,7 @@ import hashlib
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -42,10 +43,10 @@ def _headers_stamp():
     return h.hexdigest()[:12]
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
+def build(force: bool = False, verbose: bool = False, jobs: int = 0) -> Path:
     BUILD.mkdir(exist_ok=True)
     stamp = _headers_stamp()
-    objs = []
+    objs, todo = [], []
     for src in _sources():
         h = hashlib.sha1(src.read_bytes() + stamp.encode()).hexdigest()[:12]
         obj = BUILD / f"{src.stem}.{h}.o"
@@ -56,9 +57,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             cmd = [str(NVCC)] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)]
         else:
             cmd = ["g++"] + CXX_FLAGS + ["-c", str(src), "-o", str(obj)]
+        todo.append((src, cmd))
+
+    def compile_one(item):
+        src, cmd = item
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    # independent translation units: compiled concurrently (nvcc and g++ are separate processes)
+    workers = jobs or max(1, min(len(todo), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        results = list(pool.map(compile_one, todo))
+    for src, r in results:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"compile failed: {src.name}")

@@ -139,16 +139,17 @@ __device__ __forceinline__ void st_chunk(uint8_t* base, int r, int c0, int rows,
 }
 
 // D (+)= A B, operands given by descriptor bases and byte offsets; split, the low parts of A and
-// B lie a_lo / b_lo bytes after the high ones and D += A.h B.h + A.h B.l + A.l B.h
+// B lie a_lo / b_lo bytes after the high ones and D += A.h B.h + A.h B.l + A.l B.h.  Executed by
+// a whole warp (one elected lane issues).
 template <class E>
 __device__ __forceinline__ void mma(uint32_t d, const ptx::DescBase& A, uint32_t a_off, uint32_t a_lo,
                                     const ptx::DescBase& B, uint32_t b_off, uint32_t b_lo, uint32_t idesc,
                                     uint32_t acc)
 {
-  ptx::mma_bf16(d, A.at(a_off), B.at(b_off), idesc, acc);
+  ptx::mma_bf16_warp(d, A.at(a_off), B.at(b_off), idesc, acc);
   if constexpr (E::kSplit) {
-    ptx::mma_bf16(d, A.at(a_off), B.at(b_off + b_lo), idesc, 1);
-    ptx::mma_bf16(d, A.at(a_off + a_lo), B.at(b_off), idesc, 1);
+    ptx::mma_bf16_warp(d, A.at(a_off), B.at(b_off + b_lo), idesc, 1);
+    ptx::mma_bf16_warp(d, A.at(a_off + a_lo), B.at(b_off), idesc, 1);
   }
 }
 
@@ -363,43 +364,45 @@ __device__ __forceinline__ void stage_issue(const LatentBoxes& B, const Foot& f0
 }
 
 // Adds this step's quantisation noise to the staged latents of the unit's footprint (rows of
-// the boxes are B.w0 / B.w1 cells apart).
+// the boxes are B.w0 / B.w1 cells apart): the g0 box rows [r0, r1) ...
 template <class SH>
-__device__ __forceinline__ void stage_noise(const LevelArgs& L, const LatentBoxes& B, const Foot& f0, const Foot& f1,
-                                            float* foot, int gt)
+__device__ __forceinline__ void stage_noise_g0(const LevelArgs& L, const LatentBoxes& B, const Foot& f0, int r0, int r1,
+                                               float* foot, int gt)
 {
-  {
-    constexpr int C0 = SH::C0;
-    const int d0 = L.d0;
-    const int rowq = f0.w * (C0 / 4);
-    const float inv = 1.0f / (float)rowq;
-    for (int v = gt; v < f0.h * rowq; v += kGroupThreads) {
-      const int r = div_small(v, inv), q = v - r * rowq;
-      const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
-      float4* dst = reinterpret_cast<float4*>(foot + r * B.w0 * C0 + q * 4);
-      float4 val = *dst;
-      val.x += level_noise(L, 0u, (uint32_t)e);
-      val.y += level_noise(L, 0u, (uint32_t)(e + 1));
-      val.z += level_noise(L, 0u, (uint32_t)(e + 2));
-      val.w += level_noise(L, 0u, (uint32_t)(e + 3));
-      *dst = val;
-    }
+  constexpr int C0 = SH::C0;
+  const int d0 = L.d0;
+  const int rowq = f0.w * (C0 / 4);
+  const float inv = 1.0f / (float)rowq;
+  for (int v = r0 * rowq + gt; v < r1 * rowq; v += kGroupThreads) {
+    const int r = div_small(v, inv), q = v - r * rowq;
+    const int e = ((f0.y0 + r) * d0 + f0.x0) * C0 + q * 4;
+    float4* dst = reinterpret_cast<float4*>(foot + r * B.w0 * C0 + q * 4);
+    float4 val = *dst;
+    val.x += level_noise(L, 0u, (uint32_t)e);
+    val.y += level_noise(L, 0u, (uint32_t)(e + 1));
+    val.z += level_noise(L, 0u, (uint32_t)(e + 2));
+    val.w += level_noise(L, 0u, (uint32_t)(e + 3));
+    *dst = val;
   }
-  {
-    constexpr int C1 = SH::C1;
-    const int d1 = L.d1;
-    const int rowh = f1.w * (C1 / 2);
-    const float inv = 1.0f / (float)rowh;
-    float* foot1 = foot + B.g1_off + (f1.x0 & B.g1_shift) * C1;
-    for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
-      const int r = div_small(v, inv), q = v - r * rowh;
-      const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
-      float2* dst = reinterpret_cast<float2*>(foot1 + r * B.w1 * C1 + q * 2);
-      float2 val = *dst;
-      val.x += level_noise(L, 1u, (uint32_t)e);
-      val.y += level_noise(L, 1u, (uint32_t)(e + 1));
-      *dst = val;
-    }
+}
+// ... and the whole g1 box.
+template <class SH>
+__device__ __forceinline__ void stage_noise_g1(const LevelArgs& L, const LatentBoxes& B, const Foot& f1, float* foot,
+                                               int gt)
+{
+  constexpr int C1 = SH::C1;
+  const int d1 = L.d1;
+  const int rowh = f1.w * (C1 / 2);
+  const float inv = 1.0f / (float)rowh;
+  float* foot1 = foot + B.g1_off + (f1.x0 & B.g1_shift) * C1;
+  for (int v = gt; v < f1.h * rowh; v += kGroupThreads) {
+    const int r = div_small(v, inv), q = v - r * rowh;
+    const int e = ((f1.y0 + r) * d1 + f1.x0) * C1 + q * 2;
+    float2* dst = reinterpret_cast<float2*>(foot1 + r * B.w1 * C1 + q * 2);
+    float2 val = *dst;
+    val.x += level_noise(L, 1u, (uint32_t)e);
+    val.y += level_noise(L, 1u, (uint32_t)(e + 1));
+    *dst = val;
   }
 }
 
@@ -630,29 +633,53 @@ __device__ __forceinline__ void sep_pass1_g1(const float* dxs, int ld, const Cor
   *reinterpret_cast<float2*>(T1 + r * C1 + 2 * q) = sum;
 }
 
-// Loads the fp32 master weights into the canonical operand tiles (zero padding past F / C).
+// Loads the fp32 master weights into the canonical operand tiles (zero padding past F / C).  A
+// thread's 8-column chunks are all loaded (16-byte loads: F and the row offsets are multiples of
+// 4 floats) before any is converted, so the CTA waits for one round trip, not one per chunk.
 template <class SH, class E>
 __device__ void load_weights(const Model& M, uint8_t* W0, uint8_t* W1, uint8_t* Wo)
 {
   constexpr int F = SH::F, Kp = SH::Kp, kThreads = E::kGroups * kGroupThreads;
+  static_assert(F % 4 == 0, "16-byte weight loads");
+  constexpr int n0 = 64 * (Kp / 8), n1 = n0 + 64 * 8, n2 = n1 + 16 * 8;  // chunk ranges: W0, W1, Wout
+  constexpr int kPer = (n2 + kThreads - 1) / kThreads;
   const int C = M.C;
-  for (int i = threadIdx.x; i < 64 * (Kp / 8); i += kThreads) {
-    const int r = i / (Kp / 8), c0 = (i % (Kp / 8)) * 8;
-    float v[8];
-    for (int j = 0; j < 8; j++) v[j] = (c0 + j) < F ? M.W[w0_off() + r * F + c0 + j] : 0.0f;
-    st_chunk<E>(W0, r, c0, 64, Kp, v);
+  const float* __restrict__ W = M.W;
+  float4 v[kPer][2];
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const int i = (int)threadIdx.x + j * kThreads;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    v[j][0] = z;
+    v[j][1] = z;
+    const float* src = nullptr;
+    int valid = 0;  // floats of the chunk inside the matrix (0, 4 or 8)
+    if (i < n0) {
+      const int r = i / (Kp / 8), c0 = (i % (Kp / 8)) * 8;
+      src = W + w0_off() + r * F + c0;
+      valid = c0 + 8 <= F ? 8 : (c0 < F ? 4 : 0);
+    } else if (i < n1) {
+      const int r = (i - n0) >> 3, c0 = ((i - n0) & 7) * 8;
+      src = W + w1_off(F) + r * 64 + c0;
+      valid = 8;
+    } else if (i < n2) {
+      const int r = (i - n1) >> 3, c0 = ((i - n1) & 7) * 8;
+      src = W + wo_off(F) + r * 64 + c0;
+      valid = r < C ? 8 : 0;
+    }
+    if (valid >= 4) v[j][0] = __ldg(reinterpret_cast<const float4*>(src));
+    if (valid == 8) v[j][1] = __ldg(reinterpret_cast<const float4*>(src + 4));
   }
-  for (int i = threadIdx.x; i < 64 * 8; i += kThreads) {
-    const int r = i / 8, c0 = (i % 8) * 8;
-    float v[8];
-    for (int j = 0; j < 8; j++) v[j] = M.W[w1_off(F) + r * 64 + c0 + j];
-    st_chunk<E>(W1, r, c0, 64, 64, v);
-  }
-  for (int i = threadIdx.x; i < 16 * 8; i += kThreads) {
-    const int r = i / 8, c0 = (i % 8) * 8;
-    float v[8];
-    for (int j = 0; j < 8; j++) v[j] = r < C ? M.W[wo_off(F) + r * 64 + c0 + j] : 0.0f;
-    st_chunk<E>(Wo, r, c0, 16, 64, v);
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const int i = (int)threadIdx.x + j * kThreads;
+    const float c[8] = {v[j][0].x, v[j][0].y, v[j][0].z, v[j][0].w, v[j][1].x, v[j][1].y, v[j][1].z, v[j][1].w};
+    if (i < n0)
+      st_chunk<E>(W0, i / (Kp / 8), (i % (Kp / 8)) * 8, 64, Kp, c);
+    else if (i < n1)
+      st_chunk<E>(W1, (i - n0) >> 3, ((i - n0) & 7) * 8, 64, 64, c);
+    else if (i < n2)
+      st_chunk<E>(Wo, (i - n1) >> 3, ((i - n1) & 7) * 8, 16, 64, c);
   }
 }
 
@@ -781,28 +808,49 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
   uint8_t* sW1 = sW0 + tile_bytes<E>(64, Kp);
   uint8_t* sWo = sW1 + tile_bytes<E>(64, 64);
 
+  // prologue: the barriers, the step record and its level first; then the first unit's
+  // latent-box loads, in flight while the weights load and the accumulators are zeroed
+  static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
+  if (tid < (int)(sizeof(StepRec) / 4))
+    reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(T.step)[tid];
   if (tid == 0) {
     ptx::mbar_init(&bars[0], 1);
     ptx::mbar_init(&bars[1], 1);
     for (int i = 0; i < 4; i++) ptx::mbar_init(&tma_bars[i >> 1][i & 1], 1);
     ptx::fence_mbar_init();
     fail_s = 0;
+    level_s = level_args(M, *T.step);
   }
+  __syncwarp();
   if (warp == 0) ptx::tmem_alloc(&tmem_base_s, kTmemCols);
+  __syncthreads();
+  const LevelArgs& L = level_s;
+  const int ntiles = (s.texels + kTile - 1) / kTile;
+  // latent boxes: unit k's were loaded (TMA, asynchronously) while unit k-1 ran, into the
+  // staging buffer the previous unit did not use; tph holds each buffer's next wait parity and
+  // inflight which buffers have loads not yet waited for
+  const int ustride = ncta * E::kGroups;
+  Foot nf0 = {}, nf1 = {};
+  bool nstaged = false;
+  int pb = 0;
+  uint32_t tph = 0, inflight = 0;
+  {
+    const int u0 = cta * E::kGroups + g;
+    nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
+    if (nstaged) {
+      if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
+      inflight |= 1u;
+    }
+  }
   load_weights<SH, E>(M, sW0, sW1, sWo);
   if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
   // corner masks start zeroed (each unit zeroes its own after its scatter)
   static_assert(sizeof(CornerMasks) % 4 == 0, "mask words");
   for (int i = tid; i < (int)(sizeof(masks_s) / 4); i += kThreads) reinterpret_cast<uint32_t*>(masks_s)[i] = 0u;
-  static_assert(sizeof(StepRec) % 4 == 0 && sizeof(StepRec) / 4 <= kThreads, "step record copy");
-  if (tid < (int)(sizeof(StepRec) / 4))
-    reinterpret_cast<int32_t*>(&step_s)[tid] = reinterpret_cast<const int32_t*>(T.step)[tid];
   ptx::fence_proxy_async();
   ptx::fence_before_sync();
   __syncthreads();
   ptx::fence_after_sync();
-  if (tid == 0) level_s = level_args(M, s);  // published by the __syncthreads below
-  const LevelArgs& L = level_s;
   const uint32_t tbase = tmem_base_s;
   const uint32_t lane_off = (uint32_t)(quad * 32) << 16;
   // zero the shared weight-gradient accumulators (columns kColW0 .. kColWo + 16): each part
@@ -816,13 +864,13 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
 
   const uint32_t win = tbase + 128u * (uint32_t)g;    // this group's TMEM window (MMA address)
   const uint32_t lwin = win + lane_off;                // ... as seen by this thread's lane
-  const int ntiles = (s.texels + kTile - 1) / kTile;
   const float inv = -2.0f / ((float)C * (float)s.texels);  // libopenntc.cpp:666
   const uint8_t* target = M.package[s.lod];
   uint64_t* bar = &bars[g];
   uint32_t phase = 0;
   double loss = 0.0;
-  const bool issuer = gt == 0;
+  // the group's first warp issues its MMAs and commits, from one elected lane
+  const bool mma_warp = (gt >> 5) == 0;
 
   // one warp of the group polls the mbarrier; the others sleep at the group barrier
   const bool poller = (gt >> 5) == 0;
@@ -862,35 +910,24 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
   const ptx::DescBase dWok = ptx::desc_base(aWo, 128, S64), dWom = ptx::desc_base(aWo, S64, 128);
   const int hc = half * 32;  // this thread's first column of a 64-column tile
 
-  // latent boxes: unit k's were loaded (TMA, asynchronously) while unit k-1 ran, into the
-  // staging buffer the previous unit did not use; tph holds each buffer's next wait parity and
-  // inflight which buffers have loads not yet waited for
-  const int ustride = ncta * E::kGroups;
-  Foot nf0 = {}, nf1 = {};
-  bool nstaged = false;
-  int pb = 0;
-  uint32_t tph = 0, inflight = 0;
   // buffer `buf`'s boxes landed (bounded wait; a timeout is reported, the buffer stays in
-  // flight and is waited for again before exit) and, with noise, perturbed in place
-  auto land = [&](int buf, const Foot& a0, const Foot& a1) {
+  // flight and is waited for again before exit); the noise is added afterwards, in parts
+  auto land_wait = [&](int buf) {
     if (ptx::mbar_wait(&tma_bars[g][buf], (tph >> buf) & 1u)) {
       tph ^= 1u << buf;
       inflight &= ~(1u << buf);
     } else {
       atomicExch(&fail_s, 1);
     }
-    if (s.noise) stage_noise<SH>(L, boxes, a0, a1, gp.foot + buf * kFootBuf, gt);
   };
-  {
-    const int u0 = cta * E::kGroups + g;
-    nstaged = u0 < ntiles && unit_footprint<SH>(L, s, boxes, u0, nf0, nf1);
-    if (nstaged) {
-      if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot, &tma_bars[g][0]);
-      inflight |= 1u;
-      land(0, nf0, nf1);
+  if (nstaged) {  // the first unit's boxes before its gather
+    land_wait(0);
+    if (s.noise) {
+      stage_noise_g0<SH>(L, boxes, nf0, 0, nf0.h, gp.foot, gt);
+      stage_noise_g1<SH>(L, boxes, nf1, gp.foot, gt);
     }
-    bar_group(g);  // the first unit's boxes before its gather
   }
+  bar_group(g);
 
   for (int unit = cta * E::kGroups + g; unit < ntiles; unit += ustride) {
     // ------------------------------------------------------------------ gather
@@ -907,11 +944,11 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
     CornerMasks& cm = masks_s[g];
     gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < Kp / kK; k++) mma<E>(win, dXk, k * 256, kLoX, dW0k, k * 256, kLoW0, I_M128_N64_K, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     // in the shadow of the MMAs: this thread's target channels [8 half, 8 half + 8) (first
     // used after layer 2), and the next unit's box loads into the other staging buffer (its
@@ -929,7 +966,8 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
       const int nu = unit + ustride;
       nstaged = nu < ntiles && unit_footprint<SH>(L, s, boxes, nu, nf0, nf1);
       if (nstaged) {
-        if (gt == 0) stage_issue<SH>(boxes, nf0, nf1, gp.foot + (cur ^ 1) * kFootBuf, &tma_bars[g][cur ^ 1]);
+        // issued by the group's second warp: the first one issues the MMAs and polls for them
+        if (gt == 32) stage_issue<SH>(boxes, nf0, nf1, gp.foot + (cur ^ 1) * kFootBuf, &tma_bars[g][cur ^ 1]);
         inflight |= 2u >> cur;
       }
       pb ^= 1;
@@ -945,11 +983,11 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
     ptx::ld_wait();
     epi_fwd<E>(hx, h0, gp.P0, row, hc);
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < 64 / kK; k++) mma<E>(win, dP0k, k * 256, kLoP, dW1k, k * 256, kLoW1, I_M128_N64_K, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     // this unit's corner masks (zeroed at the end of the previous unit), by the group's second
     // warp while the first polls the MMA barrier
@@ -962,12 +1000,12 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
     ptx::ld_wait();
     epi_fwd<E>(hx, h1, gp.P1, row, hc);
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < 64 / kK; k++)
         mma<E>(win + 64, dP1k, k * 256, kLoP, dWok, k * 256, kLoWo, I_M128_N16_K, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
 
@@ -989,7 +1027,7 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
       st_chunk<E>(gp.dY, row, half * 8, 128, 16, d);
     }
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
       // dA1 = dY Wout: B = Wout viewed [c][h] as MN-major (N = h), K = c
 #pragma unroll
@@ -999,7 +1037,13 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
 #pragma unroll
       for (int k = 0; k < 128 / kK; k++)
         mma<E>(tbase + kColWo, dP1m, k * kKS * S64, kLoP, dYm, k * kKS * S16, kLoY, I_M64_N16_MN, 1);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
+    }
+    // the next unit's boxes (loads issued with this unit's first layer) landed, then their noise,
+    // spread over this and the next two MMA waits: the g1 box here, the g0 box's rows in halves
+    if (nstaged) {
+      land_wait(cur ^ 1);
+      if (s.noise) stage_noise_g1<SH>(L, boxes, nf1, gp.foot + (cur ^ 1) * kFootBuf, gt);
     }
     if (!wait_mma()) break;
 
@@ -1012,7 +1056,7 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
       epi_bwd<E>(da, h1, gp.P1, row, hc);
     }
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
       // dA0 = dH1 W1 : B = W1 viewed [i][h] as MN-major (N = h), K = i
 #pragma unroll
@@ -1022,9 +1066,9 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
 #pragma unroll
       for (int k = 0; k < 128 / kK; k++)
         mma<E>(tbase + kColW1, dP1m, k * kKS * S64, kLoP, dP0m, k * kKS * S64, kLoP, I_M64_N64_MN, 1);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
-    if (nstaged) land(cur ^ 1, nf0, nf1);  // the next unit's boxes, read after several barriers
+    if (nstaged && s.noise) stage_noise_g0<SH>(L, boxes, nf0, 0, nf0.h / 2, gp.foot + (cur ^ 1) * kFootBuf, gt);
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ dH0 (into P0)
@@ -1036,7 +1080,7 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
       epi_bwd<E>(da, h0, gp.P0, row, hc);
     }
     handoff();
-    if (issuer) {
+    if (mma_warp) {
       ptx::fence_after_sync();
       // dX = dH0 W0 : B = W0 viewed [h][f] as MN-major (N = f), K = h
 #pragma unroll
@@ -1046,8 +1090,10 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
 #pragma unroll
       for (int k = 0; k < 128 / kK; k++)
         mma<E>(tbase + kColW0, dP0m, k * kKS * S64, kLoP, dXm, k * kKS * SX, kLoX, I_M64_NKP_MN, 1);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
+    if (nstaged && s.noise)
+      stage_noise_g0<SH>(L, boxes, nf0, nf0.h / 2, nf0.h, gp.foot + (cur ^ 1) * kFootBuf, gt);
     if (!wait_mma()) break;
 
     // ------------------------------------------------------------------ scatter dX
