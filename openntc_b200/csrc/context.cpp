@@ -1152,10 +1152,10 @@ int ontc_load_manifest(ontc_context* c, const char* path)
 
   // Mip chains per source (libopenntc.cpp:1296-1336)
   const size_t n0 = (size_t)dim * dim;
-  DBuf<uint8_t> rgba_dev, chain[ONTC_MAX_MIPS];
-  DBuf<float> tmp;
+  DBuf<uint8_t> rgba_dev;
   std::vector<DBuf<uint8_t>> src_mips((size_t)count * c->mips);
-  if (rgba_dev.alloc(n0 * 4) || tmp.alloc(n0 * 2)) return fail(ONTC_ALLOCATION_FAILURE);
+  if (rgba_dev.alloc(n0 * 4)) return fail(ONTC_ALLOCATION_FAILURE);
+  int pkg_off = 0;  // the source's first channel in the target package (sources in package order)
   std::string base_dir;
   {
     std::string p(path);
@@ -1179,15 +1179,19 @@ int ontc_load_manifest(ontc_context* c, const char* path)
     for (int m = 0; m < c->mips; m++)
       if (src_mips[(size_t)i * c->mips + m].alloc((size_t)c->mip_dim[m] * c->mip_dim[m] * s.nch))
         return fail(ONTC_ALLOCATION_FAILURE);
-    if (launch_prepare(rgba_dev.p, (int)dim, s.cmap, s.nch, src_mips[(size_t)i * c->mips].p, c->stream))
+    // the chain fused with packaging: each mip of this source is written once, into the
+    // source's mip and into its channels of that mip's target package (libopenntc.cpp:1338-1362)
+    if (launch_prepare_package(rgba_dev.p, (int)dim, s.cmap, s.nch, src_mips[(size_t)i * c->mips].p, c->package[0].p,
+                               c->C, pkg_off, c->stream))
       return fail(ONTC_CUDA_FAILURE);
     c->launches++;
     for (int m = 1; m < c->mips; m++) {
-      if (launch_lanczos_down(src_mips[(size_t)i * c->mips + m - 1].p, c->mip_dim[m - 1], s.nch, tmp.p,
-                              src_mips[(size_t)i * c->mips + m].p, c->stream))
+      if (launch_lanczos_down_package(src_mips[(size_t)i * c->mips + m - 1].p, c->mip_dim[m - 1], s.nch,
+                                      src_mips[(size_t)i * c->mips + m].p, c->package[m].p, c->C, pkg_off, c->stream))
         return fail(ONTC_CUDA_FAILURE);
-      c->launches += 2;
+      c->launches++;
     }
+    pkg_off += s.nch;
     for (int m = 0; m < c->mips; m++) {
       c->mips_host[i][m].assign((size_t)c->mip_dim[m] * c->mip_dim[m] * s.nch, 0);
       if (cudaMemcpyAsync(c->mips_host[i][m].data(), src_mips[(size_t)i * c->mips + m].p, c->mips_host[i][m].size(),
@@ -1196,23 +1200,7 @@ int ontc_load_manifest(ontc_context* c, const char* path)
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(ONTC_CUDA_FAILURE);
   }
-  // Channel interleave into the per-mip target package (libopenntc.cpp:1338-1362)
-  PackageSpec spec = {};
-  int p = 0;
-  for (int j2 = 0; j2 < count; j2++) {
-    spec.src_channels[j2] = c->sources[j2].nch;
-    for (int ch = 0; ch < c->sources[j2].nch; ch++) {
-      spec.feat_src[p] = j2;
-      spec.feat_chan[p] = ch;
-      p++;
-    }
-  }
-  if (p != c->C) return fail(ONTC_INVALID_MANIFEST);
-  for (int m = 0; m < c->mips; m++) {
-    for (int j2 = 0; j2 < count; j2++) spec.src[j2] = src_mips[(size_t)j2 * c->mips + m].p;
-    if (launch_package(spec, c->mip_dim[m], c->C, c->package[m].p, c->stream)) return fail(ONTC_CUDA_FAILURE);
-    c->launches++;
-  }
+  if (pkg_off != c->C) return fail(ONTC_INVALID_MANIFEST);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(ONTC_CUDA_FAILURE);
   c->train_phase = ONTC_MANIFEST_LOADED;
   return ONTC_SUCCESS;

@@ -177,18 +177,16 @@ cudaError_t launch_noise_init(void* states, int n_states, cudaStream_t stream);
 cudaError_t launch_noise_fill(void* states, int n_states, long long n, float delta, float* out, cudaStream_t stream);
 
 // ---- mip chain (LoadManifest)
-// picks `cmap_count` channels (cmap[i] in 0..3) out of an RGBA8 image into [dim][dim][count]
-cudaError_t launch_prepare(const uint8_t* rgba, int dim, const int* cmap, int count, uint8_t* out, cudaStream_t stream);
-// one separable Lanczos-3 2x reduction [dim][dim][c] -> [dim/2][dim/2][c]; tmp holds dim*dim/2*c floats
+// one separable Lanczos-3 2x reduction [dim][dim][c] -> [dim/2][dim/2][c] in two kernels; tmp
+// holds dim*dim/2*c floats (the caller-buffer entry points; LoadManifest uses the fused chain)
 cudaError_t launch_lanczos_down(const uint8_t* src, int dim, int c, float* tmp, uint8_t* dst, cudaStream_t stream);
-// interleaves the sources' channels into the [dim][dim][C] target package
-struct PackageSpec {
-  const uint8_t* src[16];
-  int32_t src_channels[16];
-  int32_t feat_src[16];
-  int32_t feat_chan[16];
-};
-cudaError_t launch_package(const PackageSpec& spec, int dim, int C, uint8_t* out, cudaStream_t stream);
+// The ingest chain fused with packaging: mip 0 of a source (channel selection) and each 2x
+// reduction (both Lanczos passes in one kernel) also write the source's channels
+// [pkg_off, pkg_off + count) of that mip's target package [dim][dim][C].
+cudaError_t launch_prepare_package(const uint8_t* rgba, int dim, const int* cmap, int count, uint8_t* out, uint8_t* pkg,
+                                   int C, int pkg_off, cudaStream_t stream);
+cudaError_t launch_lanczos_down_package(const uint8_t* src, int dim, int c, uint8_t* dst, uint8_t* pkg, int C,
+                                        int pkg_off, cudaStream_t stream);
 // the 12 Lanczos-3 tap weights as the filter computes them (test hook)
 cudaError_t lanczos_weights(float* host12);
 
