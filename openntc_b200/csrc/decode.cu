@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
   const uint32_t lwin = win + ((uint32_t)(quad * 32) << 16);
   uint64_t* bar = &bars[g];
   uint32_t phase = 0;
-  const bool issuer = row == 0, poller = (row >> 5) == 0;
+  // the group's first warp issues its MMAs (one elected lane) and polls for them
+  const bool issuer = (row >> 5) == 0, poller = issuer;
   const int C = A.k.channel_count;
   const float rcp1 = A.k.rcp_s_a1, rcp2 = A.k.rcp_s_a2;
   const bool fast1 = rcp1 >= 1.6e-5f && rcp1 <= 600.0f, fast2 = rcp2 >= 1.6e-5f && rcp2 <= 600.0f;
@@ -550,8 +551,8 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < Kp / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, 1);
-      ptx::commit(bar);
+        ptx::mma_s8_warp(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, 1);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a0 -> A (over X)
@@ -561,8 +562,8 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < kHid / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, 1);
-      ptx::commit(bar);
+        ptx::mma_s8_warp(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, 1);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a1 -> A
@@ -572,8 +573,8 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::fence_after_sync();
 #pragma unroll
       for (int k = 0; k < kHid / 32; k++)
-        ptx::mma_s8(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, 1);
-      ptx::commit(bar);
+        ptx::mma_s8_warp(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, 1);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- outputs

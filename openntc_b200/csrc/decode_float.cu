@@ -213,11 +213,12 @@ __host__ __device__ constexpr uint32_t idesc_e4m3(int M, int N)
   return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// issued by the lane elect.sync picks in a converged warp, as ptx::mma_bf16_warp
 __device__ __forceinline__ void mma_e4m3(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
 {
   asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
-          d_tmem),
+      "{\n\t.reg .pred p, e;\n\telect.sync _|e, 0xffffffff;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
@@ -318,7 +319,8 @@ __global__ void __launch_bounds__(kTThreads, 1) decode_tc_kernel(const __grid_co
   const uint32_t lwin = win + ((uint32_t)(quad * 32) << 16);
   uint64_t* bar = &bars[g];
   uint32_t phase = 0;
-  const bool issuer = row == 0, poller = (row >> 5) == 0;
+  // the group's first warp issues its MMAs (one elected lane) and polls for them
+  const bool issuer = (row >> 5) == 0, poller = issuer;
   const int C = A.k.channel_count;
   const float inv_sx = 1.0f / A.sx, pre0 = A.sx * A.sw0, post0 = 1.0f / A.sa1;
   const float pre1 = A.sa1 * A.sw1, post1 = 1.0f / A.sa2, outs = A.sa2 * A.swo;
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(kTThreads, 1) decode_tc_kernel(const __grid_co
     if constexpr (FP8)
       mma_e4m3(d, a, b, id, acc);
     else
-      ptx::mma_bf16(d, a, b, id, acc);
+      ptx::mma_bf16_warp(d, a, b, id, acc);
   };
   auto wait_mma = [&]() -> bool {
     if (poller && !ptx::mbar_wait(bar, phase)) atomicExch(&fail_s, 1);
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(kTThreads, 1) decode_tc_kernel(const __grid_co
 #pragma unroll
       for (int k = 0; k < Kp / KSTEP; k++)
         mma(win, ptx::desc(aX + k * 256, 128, SX), ptx::desc(aW0 + k * 256, 128, SX), I_L01, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a0 -> X
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(kTThreads, 1) decode_tc_kernel(const __grid_co
 #pragma unroll
       for (int k = 0; k < 64 / KSTEP; k++)
         mma(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aW1 + k * 256, 128, S64), I_L01, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- a1 -> X
@@ -397,7 +399,7 @@ __global__ void __launch_bounds__(kTThreads, 1) decode_tc_kernel(const __grid_co
 #pragma unroll
       for (int k = 0; k < 64 / KSTEP; k++)
         mma(win, ptx::desc(aX + k * 256, 128, S64), ptx::desc(aWo + k * 256, 128, S64), I_L2, k > 0);
-      ptx::commit(bar);
+      ptx::commit_warp(bar);
     }
     if (!wait_mma()) break;
     // ---------------------------------------------------------------- outputs
