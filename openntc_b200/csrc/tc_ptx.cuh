@@ -184,32 +184,11 @@ __host__ __device__ constexpr uint32_t idesc_s8(int M, int N, bool a_mn, bool b_
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
-{
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
-          d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
-{
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
-          d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void commit(uint64_t* bar)
-{
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
-               : "memory");
-}
-
-// The same three operations executed by a whole converged warp, issued by the one lane that
-// elect.sync picks (the lowest active lane, so the MMAs and the commit that tracks them come
-// from the same thread).  The warp's control flow stays uniform, so the descriptor operands
-// are warp-uniform values rather than one divergent thread's registers.
+// MMAs (kind::f16 with bf16 operands, kind::i8) and the commit that tracks them, executed by a
+// whole converged warp and issued by the one lane that elect.sync picks (the lowest active lane,
+// so the MMAs and their commit come from the same thread).  The warp's control flow stays
+// uniform, so the descriptor operands are warp-uniform values rather than one divergent
+// thread's registers.
 __device__ __forceinline__ void mma_bf16_warp(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                               uint32_t accumulate)
 {
