@@ -23,8 +23,9 @@ stream (max over ranks): K-step regions, each between a barrier and a synchroniz
 until at least 1 s of device time, median region; `e2e` is the same steps through the C ABI
 timed on the host, including the per-step draw upload and the read-back of every step's loss.
 On one GPU the default line also carries the metric's other parts: `s_to_psnr` (training
-seconds until the Eval PSNR first reaches a stated target over the whole schedule) and `decode`
-(the decode workload through the int8 decoder, as `--workload decode` prints it).
+seconds until the Eval PSNR first reaches a stated target over the whole schedule), `decode`
+(the decode workload through the int8 decoder, as `--workload decode` prints it) and `batch`
+(the 16-material workload, as `--workload batch` prints it).
 --impl reference times upstream's own Context::Train built from its sources (oracle/_ref),
 with its own s-to-PSNR run on the same set and schedule.
 """
@@ -335,9 +336,11 @@ def run_ours(args):
     ctx.destroy()
     if rank == 0 and world == 1 and not args.no_extras:
         # the metric's other parts, measured in the same run: seconds to a stated PSNR over the
-        # whole schedule, and the decode workload through the int8 decoder
+        # whole schedule, the decode workload through the int8 decoder
         out["s_to_psnr"] = s_to_psnr_ours(manifest, stream, precision, latent_adam)
         out["decode"] = run_decode(args, embedded=True)
+        # and the 16-material batch (many materials of uneven size, channels and profile)
+        out["batch"] = run_batch(args, embedded=True)
     if rank == 0:
         print(json.dumps(out), flush=True)
     group.barrier()
@@ -588,16 +591,20 @@ def batch_materials():
              "seed": 10 + i} for i in range(16)]
 
 
-def run_batch(args):
-    """16 uneven materials trained together (ontc_train_batch: each context on its own stream,
-    their step chunks interleaved) against each trained alone for the same steps."""
+def run_batch(args, embedded=False):
+    """16 uneven materials trained together (ontc_train_batch: BF16 contexts in lock step, one
+    shared tile launch per profile shape and step) against each trained alone for the same steps.
+    `embedded`: measured inside the default training run (its sub-object), on the current GPU."""
     import torch
     import openntc_b200 as ont
     from openntc_b200.synth import make_material
-    world, rank, local = dist_setup(args)
-    if rank != 0:
-        return None
-    torch.cuda.set_device(local)
+    if embedded:
+        local = torch.cuda.current_device()
+    else:
+        world, rank, local = dist_setup(args)
+        if rank != 0:
+            return None
+        torch.cuda.set_device(local)
     tmp = Path(tempfile.mkdtemp(prefix="ontc_batch_"))
     mats = batch_materials()
     manifests = [make_material(tmp / f"m{i}", m["dim"], m["seed"], m["channels"]) for i, m in enumerate(mats)]
@@ -652,7 +659,8 @@ def run_batch(args):
         "max_psnr_difference_db": round(max(abs(a - b) for a, b in zip(psnr_batch, alone)), 4),
         "clocks": clk.summary(), "impl": "ours",
     }
-    print(json.dumps(out), flush=True)
+    if not embedded:
+        print(json.dumps(out), flush=True)
     return out
 
 
