@@ -123,9 +123,11 @@ __global__ void __launch_bounds__(256) lanczos_down_package_kernel(const uint8_t
                                                                    int C, int pkg_off)
 {
   __shared__ float w[12];
+  __shared__ float unit[256];  // v / 255 for every byte v, divided once (correctly rounded, as per tap)
   __shared__ float xs[kTileRows][kTileO][CH];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;  // 32 x 8 threads
   if (tid < 12) w[tid] = lanczos_tap(tid - 6);
+  unit[tid] = __fdiv_rn((float)tid, 255.0f);
   __syncthreads();
   const int odim = dim >> 1;
   const int ox0 = blockIdx.x * kTileO, oy0 = blockIdx.y * kTileO;
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(256) lanczos_down_package_kernel(const uint8_t
       const int sx = center + i;
       if (sx < 0 || sx >= dim) continue;
       const float wt = w[i + 6];
-      for (int j = 0; j < c && j < CH; j++) total[j] = __fmaf_rn(__fdiv_rn((float)row[sx * c + j], 255.0f), wt, total[j]);
+      for (int j = 0; j < c && j < CH; j++) total[j] = __fmaf_rn(unit[row[sx * c + j]], wt, total[j]);
       tw = __fadd_rn(tw, wt);
     }
     for (int j = 0; j < c && j < CH; j++) xs[r][k % kTileO][j] = __fdiv_rn(total[j], tw);
