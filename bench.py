@@ -281,7 +281,10 @@ def run_ours(args):
                  "avg_launch_us": per_launch(adam), "share_of_step": round(adam.total_ms / step_total, 3),
                  "traffic": traffic_tab.get("footprint_update_main_bytes_per_launch"
                                             if latent_adam == ont.LatentAdam.DEFERRED
-                                            else "adam_step_bytes_per_launch")},
+                                            else "adam_step_bytes_per_launch"),
+                 "traffic_note": ("traffic: one launch of a lod-0 step captured by ncu with cold caches; "
+                                  "algorithmic_bytes_per_launch: the mean over this run's steps, whose "
+                                  "footprints grow with the lod (a lod-2 step's is the whole level)")},
         "catchup": {"name": "catchup_kernel + sweep_kernel (zero-gradient replay)", "bound": "hbm",
                     "achieved": round(gbs(catchup), 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "launches_per_step": catchup.launches / K, "avg_launch_us": per_launch(catchup),
