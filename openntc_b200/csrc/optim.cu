@@ -105,6 +105,36 @@ __device__ __forceinline__ void decoder_block(const Model& M, const StepRec& s, 
   M.Wv[w] = v;
 }
 
+// Decoder Adam when the gradient is the one row the tcgen05 tile kernels add into: one thread per
+// weight (CTA `blk` of the decoder part takes weights [256 blk, 256 blk + 256)), the row read and
+// zeroed for the next step; CTA 0's first warp also reduces the `grid` loss partials.
+constexpr int kDecRowWeights = 256;
+__device__ __forceinline__ void decoder_row_block(const Model& M, const StepRec& s, int blk, float* __restrict__ dW,
+                                                  const double* __restrict__ loss_partial, int grid,
+                                                  double* __restrict__ loss_out)
+{
+  const int lane = threadIdx.x & 31;
+  if (blk == 0 && threadIdx.x < 32) {
+    double l = 0.0;
+    for (int i = lane; i < grid; i += 32) l += loss_partial[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if (lane == 0 && loss_out) loss_out[s.step] = l / ((double)M.C * (double)s.texels);
+  }
+  // upstream updates all of W0, W1 and the first C rows of Wout (libopenntc.cpp:722-754)
+  const int nupd = min(M.nW, wo_off(M.F) + M.C * kHidden);
+  const int w = blk * kDecRowWeights + (int)threadIdx.x;
+  if (w >= M.nW) return;
+  const float g = dW[w];
+  dW[w] = 0.0f;  // the row is zero whenever a tile kernel starts
+  if (w >= nupd) return;
+  float p = M.W[w], m = M.Wm[w], v = M.Wv[w];
+  adam1(p, m, v, g, s.lr_dec, s.b1, s.b2);
+  M.W[w] = p;
+  M.Wm[w] = m;
+  M.Wv[w] = v;
+}
+
 // ---- deferred latent optimiser ------------------------------------------------------------
 // Dense Adam touches every latent of the level every step.  Here a latent cell remembers how
 // many level steps it has received: max(applied[cell], floor), where the floor is the level
@@ -270,7 +300,10 @@ __global__ void __launch_bounds__(256)
 {
   const StepRec& s = steps[idx];
   if ((int)blockIdx.x < n_dec) {
-    decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
+    if (dw_acc)
+      decoder_row_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
+    else
+      decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
     return;
   }
   const int lvl = s.level, j = s.gstep;
@@ -301,7 +334,10 @@ __global__ void __launch_bounds__(256) adam_step_kernel(Model M, const StepRec* 
 {
   const StepRec& s = steps[step_idx];
   if ((int)blockIdx.x < n_dec_blocks) {
-    decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
+    if (dw_acc)
+      decoder_row_block(M, s, blockIdx.x, dW_partial, loss_partial, grid, loss_out);
+    else
+      decoder_block(M, s, blockIdx.x, dW_partial, dw_acc, loss_partial, grid, loss_out);
     return;
   }
   if (!s.grid_update) return;
@@ -402,7 +438,9 @@ cudaError_t launch_footprint_update(const Model& M, const StepRec* d_steps, int 
                                     bool decoder, float* dW_partial, bool dw_acc, const double* loss_partial, int grid,
                                     double* loss_out, cudaStream_t stream)
 {
-  const int n_dec = decoder ? dec_blocks(M) : 0;
+  // the row gradient of the tcgen05 tile kernels: one thread per weight; per-CTA partials: 32
+  // weights per CTA, summed by its eight warps
+  const int n_dec = !decoder ? 0 : dw_acc ? (M.nW + kDecRowWeights - 1) / kDecRowWeights : dec_blocks(M);
 #define X(a, b)                                                                                          \
   if (M.g0.channels == a && M.g1.channels == b) {                                                        \
     const int total = F.cells[0] * Groups<a>::Q + F.cells[1] * Groups<b>::Q;                             \
@@ -454,7 +492,7 @@ cudaError_t launch_adam_step(const Model& M, const StepRec* d_steps, int step_id
 {
   // Sized for the largest level so one launch shape serves every step; CTAs beyond the
   // step level's work exit at once.
-  const int n_dec = dec_blocks(M);
+  const int n_dec = dw_acc ? (M.nW + kDecRowWeights - 1) / kDecRowWeights : dec_blocks(M);
   const long long n0 = (long long)M.g0.dim[0] * M.g0.dim[0] * M.g0.channels;
   const long long n1 = (long long)M.g1.dim[0] * M.g1.dim[0] * M.g1.channels;
   long long quads = (n0 + n1) / 4;
