@@ -481,7 +481,7 @@ __device__ __noinline__ void gather_half_direct(LevelArgs L, int x, int y, int r
 template <class SH, class E>
 __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxes& B, int x, int y, bool valid, int row,
                                            int half, bool staged, const Foot& f0, const Foot& f1, const float* foot,
-                                           uint8_t* sX)
+                                           const float (*penc)[8], uint8_t* sX)
 {
   constexpr int C0 = SH::C0, C1 = SH::C1, Kp = SH::Kp;
   constexpr int kSplit = 4 * C0;  // a multiple of 8: chunk-aligned
@@ -540,8 +540,15 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxe
   }
 #pragma unroll
   for (int c = 0; c < C1; c++) put(acc[c]);
-#pragma unroll
-  for (int i = 0; i < 12; i++) put(pos_enc(x, y, i));
+  // the 12 triangle waves from the per-CTA table (their values depend on the coordinate mod 8 only):
+  // per period, x phase 0, x phase 1, y phase 0, y phase 1 (pos_enc's feature order)
+  {
+    const float4 ax = *reinterpret_cast<const float4*>(penc[x & 7]), ay = *reinterpret_cast<const float4*>(penc[y & 7]);
+    const float2 bx = *reinterpret_cast<const float2*>(penc[x & 7] + 4), by = *reinterpret_cast<const float2*>(penc[y & 7] + 4);
+    put(ax.x), put(ax.y), put(ay.x), put(ay.y);
+    put(ax.z), put(ax.w), put(ay.z), put(ay.w);
+    put(bx.x), put(bx.y), put(by.x), put(by.y);
+  }
   put(L.norm_lod);
 #pragma unroll
   for (int i = 4 * C0 + C1 + 13; i < Kp; i++) put(0.0f);
@@ -779,6 +786,9 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
   __shared__ int fail_s;
   __shared__ double red[kThreads / 32];
   __shared__ float u8_to_unit[256];  // v / 255 as upstream computes it (libopenntc draw_targets)
+  // triangle-wave features of a texel coordinate c, by c mod 8: [period p][phase h] at 2p + h,
+  // pos_enc's exact values (its periods 8, 4, 2 divide 8)
+  __shared__ __align__(16) float penc_s[8][8];
   __shared__ CornerMasks masks_s[2];
   __shared__ StepRec step_s;
   __shared__ LevelArgs level_s;
@@ -844,6 +854,10 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
   }
   load_weights<SH, E>(M, sW0, sW1, sWo);
   if (tid < 256) u8_to_unit[tid] = (float)tid / 255.0f;
+  if (tid < 48) {
+    const int m = tid / 6, k = tid % 6;                 // coordinate mod 8, 2 x period + phase
+    penc_s[m][k] = pos_enc(m, m, 4 * (k >> 1) + (k & 1));  // feature 4p + h: the x wave of period p
+  }
   // corner masks start zeroed (each unit zeroes its own after its scatter)
   static_assert(sizeof(CornerMasks) % 4 == 0, "mask words");
   for (int i = tid; i < (int)(sizeof(masks_s) / 4); i += kThreads) reinterpret_cast<uint32_t*>(masks_s)[i] = 0u;
@@ -942,7 +956,7 @@ __global__ void __launch_bounds__(E::kGroups * kGroupThreads, 1) tc_unit_kernel(
     const int cur = pb;
     float* foot = gp.foot + cur * kFootBuf;
     CornerMasks& cm = masks_s[g];
-    gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, gp.X);
+    gather_half<SH, E>(L, boxes, x, y, valid, row, half, staged, f0, f1, foot, penc_s, gp.X);
     handoff();
     if (mma_warp) {
       ptx::fence_after_sync();
