@@ -215,13 +215,13 @@ __device__ __forceinline__ float level_noise(const LevelArgs& L, uint32_t which,
 
 // hardgelu of 8 fp32 accumulator values, computed on packed bf16 pairs (the results feed the next
 // bf16 MMA, so they are bf16 either way), as one 16-byte chunk of activations:
-//   c = clamp(x, -1.5, 1.5);  hg = c * (c + 1.5) * (1/3) + max(x - 1.5, 0)
+//   c = clamp(x, -1.5, 1.5);  hg = c * (c + 1.5) * (1/3) + relu(x - 1.5)
 // (the second term is x - 1.5 above the knee, where c = 1.5 and the first term is 1.5).
 __device__ __forceinline__ uint4 hg_chunk_bf16(const float* x, uint32_t* pre)
 {
   const __nv_bfloat162 lo = __floats2bfloat162_rn(-1.5f, -1.5f), hi = __floats2bfloat162_rn(1.5f, 1.5f);
   const __nv_bfloat162 third = __floats2bfloat162_rn(1.0f / 3.0f, 1.0f / 3.0f);
-  const __nv_bfloat162 zero = __floats2bfloat162_rn(0.0f, 0.0f);
+  const __nv_bfloat162 one = __floats2bfloat162_rn(1.0f, 1.0f), mhi = __floats2bfloat162_rn(-1.5f, -1.5f);
   uint32_t w[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) {
@@ -229,7 +229,8 @@ __device__ __forceinline__ uint4 hg_chunk_bf16(const float* x, uint32_t* pre)
     pre[i] = *reinterpret_cast<const uint32_t*>(&v);  // kept for the backward pass
     const __nv_bfloat162 c = __hmin2(__hmax2(v, lo), hi);
     const __nv_bfloat162 mid = __hmul2(__hmul2(c, __hadd2(c, hi)), third);
-    const __nv_bfloat162 r = __hadd2(mid, __hmax2(__hsub2(v, hi), zero));
+    // max(v - 1.5, 0) in one fused operation: v * 1 is exact, so the one rounding is that of v - 1.5
+    const __nv_bfloat162 r = __hadd2(mid, __hfma2_relu(v, one, mhi));
     w[i] = *reinterpret_cast<const uint32_t*>(&r);
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
