@@ -498,20 +498,22 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxe
     return;
   }
   const int d0 = L.d0, d1 = L.d1;
-  const int l0 = log2_pow2(d0), l1 = log2_pow2(d1);
-  Gather G;
-  gather_geometry(x, y, L.mip_dim, d0, d1, G);
+  // gather_geometry's arithmetic, each half for its own grid only: the corner cells' (x, y),
+  // clamped into the grid, and for g1 the bilinear weights
+  const float rm = rcp_pow2(L.mip_dim);  // exact: (x + 0.5) / mip_dim
+  const float u = ((float)x + 0.5f) * rm, v = ((float)y + 0.5f) * rm;
   float buf[8];
   int f = 0;  // features put so far (compile-time after unrolling, so buf stays in registers)
-  auto put = [&](float v) {
-    buf[f & 7] = v;
+  auto put = [&](float val) {
+    buf[f & 7] = val;
     f++;
     if ((f & 7) == 0) st_chunk<E>(sX, row, col0 + f - 8, 128, Kp, buf);
   };
   if (half == 0) {
+    const int gx = (int)floorf(u * (float)d0 - 0.5f), gy = (int)floorf(v * (float)d0 - 0.5f);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const int cy = G.c0[k] >> l0, cx = G.c0[k] & (d0 - 1);
+      const int cx = clampi(gx + (k & 1), 0, d0 - 1), cy = clampi(gy + (k >> 1), 0, d0 - 1);
       const float* src = foot + ((cy - f0.y0) * B.w0 + (cx - f0.x0)) * C0;
 #pragma unroll
       for (int c = 0; c < C0; c += 4) {
@@ -524,19 +526,24 @@ __device__ __forceinline__ void gather_half(const LevelArgs& L, const LatentBoxe
     }
     return;
   }
+  const float g1x = u * (float)d1 - 0.5f, g1y = v * (float)d1 - 0.5f;
+  const float fx1 = floorf(g1x), fy1 = floorf(g1y);
+  const int gx = (int)fx1, gy = (int)fy1;
+  const float g1xf = g1x - fx1, g1yf = g1y - fy1;
+  const float w1[4] = {(1.0f - g1xf) * (1.0f - g1yf), g1xf * (1.0f - g1yf), (1.0f - g1xf) * g1yf, g1xf * g1yf};
   float acc[C1];
 #pragma unroll
   for (int c = 0; c < C1; c++) acc[c] = 0.0f;
   const float* foot1 = foot + B.g1_off + (f1.x0 & B.g1_shift) * C1;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    const int cy = G.c1[k] >> l1, cx = G.c1[k] & (d1 - 1);
+    const int cx = clampi(gx + (k & 1), 0, d1 - 1), cy = clampi(gy + (k >> 1), 0, d1 - 1);
     const float* src = foot1 + ((cy - f1.y0) * B.w1 + (cx - f1.x0)) * C1;
 #pragma unroll
     for (int c = 0; c < C1; c += 2) {
       const float2 q = *reinterpret_cast<const float2*>(src + c);
-      acc[c] = __fmaf_rn(G.w1[k], q.x, acc[c]);
-      acc[c + 1] = __fmaf_rn(G.w1[k], q.y, acc[c + 1]);
+      acc[c] = __fmaf_rn(w1[k], q.x, acc[c]);
+      acc[c + 1] = __fmaf_rn(w1[k], q.y, acc[c + 1]);
     }
   }
 #pragma unroll
