@@ -243,11 +243,19 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
         blend[c / 2] = ptx::fma2(m2, centred, blend[c / 2]);
       }
     }
+    // the g1 bytes start on a word boundary (4 C0): whole words by byte permutes, a last pair
+    // (C1 = 10) byte by byte
+    static_assert((4 * C0) % 4 == 0 && C1 % 2 == 0, "g1 feature bytes");
+    uint32_t b[C1];
 #pragma unroll
     for (int c = 0; c < C1; c += 2) {
-      put_byte(w, 4 * C0 + c, (int)s8_rne_sat(__fmul_rn(blend[c / 2].x, 128.0f)));
-      put_byte(w, 4 * C0 + c + 1, (int)s8_rne_sat(__fmul_rn(blend[c / 2].y, 128.0f)));
+      b[c] = s8_rne_sat(__fmul_rn(blend[c / 2].x, 128.0f));
+      b[c + 1] = s8_rne_sat(__fmul_rn(blend[c / 2].y, 128.0f));
     }
+#pragma unroll
+    for (int c = 0; c + 4 <= C1; c += 4) w[(4 * C0 + c) >> 2] = pack4(b[c], b[c + 1], b[c + 2], b[c + 3]);
+#pragma unroll
+    for (int c = C1 & ~3; c < C1; c++) put_byte(w, 4 * C0 + c, (int)b[c]);
   }
   // 12 triangle waves of the texel coordinate at this lod, then the normalised lod
   {
