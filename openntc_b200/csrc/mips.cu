@@ -1,5 +1,8 @@
-// Manifest ingest kernels: channel selection, the separable Lanczos-3 2x mip reduction and
-// the interleaved target package (upstream ntc_kernel.cu:533-686, libopenntc.cpp:1296-1362).
+// Manifest ingest kernels (upstream ntc_kernel.cu:533-686, libopenntc.cpp:1296-1362): the mip
+// chain fused with packaging -- mip 0's channel selection and every separable Lanczos-3 2x
+// reduction (both passes in one kernel through a shared-memory tile) write a source's mip and
+// its channels of that mip's interleaved target package -- and the two-kernel reduction through
+// an fp32 intermediate that the caller-buffer entry points use.
 //
 // The reduction must reproduce upstream's u8 mips exactly (the training targets and the
 // .ntc size/PSNR depend on them), so its arithmetic follows filter_lanczos op for op:
