@@ -234,12 +234,25 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
       uint32_t st[(C1 * B1 + 31) / 32];
       cell_stream<C1 * B1>(A.g1, A.g1_words, o1, (uint32_t)(cy * d1 + cx), st);
       const float2 m2 = make_float2(mh[q], mh[q]);
+      static_assert(B1 == 4, "4-bit g1 codes (every profile)");
+      // each word's even and odd codes as bytes, masked once per word: code c (nibble c mod 8 of
+      // word c / 8) is byte (c mod 8) / 2 of lo (c even) or hi (c odd)
+      constexpr int NW1 = (C1 * B1 + 31) / 32;
+      uint32_t lo[NW1], hi[NW1];
+#pragma unroll
+      for (int j = 0; j < NW1; j++) {
+        lo[j] = st[j] & 0x0F0F0F0Fu;
+        hi[j] = (st[j] >> 4) & 0x0F0F0F0Fu;
+      }
 #pragma unroll
       for (int c = 0; c < C1; c += 2) {
-        // code - half, exactly, for two channels; then the weighted blend on the pair
-        const float2 centred = ptx::add2(make_float2(__uint_as_float(0x4B000000u | code_of<B1>(st, c)),
-                                                     __uint_as_float(0x4B000000u | code_of<B1>(st, c + 1))),
-                                         off);
+        // the float bits 0x4B000000 | code by one byte permute (byte 0 the code, bytes 1-2 zero,
+        // byte 3 0x4B), then code - half, exactly, for the two channels; then the weighted blend
+        const uint32_t sel = 0x7540u | (uint32_t)((c & 7) >> 1);
+        const float2 centred =
+            ptx::add2(make_float2(__uint_as_float(__byte_perm(lo[c >> 3], 0x4B000000u, sel)),
+                                  __uint_as_float(__byte_perm(hi[c >> 3], 0x4B000000u, sel))),
+                      off);
         blend[c / 2] = ptx::fma2(m2, centred, blend[c / 2]);
       }
     }
