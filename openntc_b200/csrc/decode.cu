@@ -205,8 +205,21 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
       uint32_t st[(C0 * B0 + 31) / 32];
       cell_stream<C0 * B0>(A.g0, A.g0_words, o0, (uint32_t)(cy * d0 + cx), st);
       static_assert(C0 % 4 == 0, "g0 features fill whole words");
+      if constexpr (B0 == 4) {
+        // a whole word of eight codes at once: even codes into the high nibble of each byte, odd
+        // ones likewise, each byte (code << 4) ^ 0x80, interleaved by two byte permutes
 #pragma unroll
-      for (int c = 0; c < C0; c += 4) w[(q * C0 + c) >> 2] = code_bytes4<B0>(st, c);
+        for (int c = 0; c + 8 <= C0; c += 8) {
+          const uint32_t t = st[c >> 3];
+          const uint32_t ev = ((t << 4) & 0xF0F0F0F0u) ^ 0x80808080u, od = (t & 0xF0F0F0F0u) ^ 0x80808080u;
+          w[(q * C0 + c) >> 2] = __byte_perm(ev, od, 0x5140);
+          w[(q * C0 + c + 4) >> 2] = __byte_perm(ev, od, 0x7362);
+        }
+        if constexpr (C0 % 8 == 4) w[(q * C0 + C0 - 4) >> 2] = code_bytes4<B0>(st, C0 - 4);
+      } else {
+#pragma unroll
+        for (int c = 0; c < C0; c += 4) w[(q * C0 + c) >> 2] = code_bytes4<B0>(st, c);
+      }
     }
   }
   // g1: bilinear blend of the dequantised codes, then *128 to a signed byte
