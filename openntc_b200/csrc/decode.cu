@@ -217,8 +217,21 @@ __device__ __forceinline__ void features(const DecodeArgs& A, float u, float v, 
         }
         if constexpr (C0 % 8 == 4) w[(q * C0 + C0 - 4) >> 2] = code_bytes4<B0>(st, C0 - 4);
       } else {
-#pragma unroll
-        for (int c = 0; c < C0; c += 4) w[(q * C0 + c) >> 2] = code_bytes4<B0>(st, c);
+        // 2-bit codes (C0 <= 16: one word): plane i holds code 4k + i in byte k, already as
+        // (code << 6) ^ 0x80; a 4 x 4 byte transpose by byte permutes gives feature word k =
+        // codes 4k .. 4k + 3
+        static_assert(B0 == 2 && C0 <= 16, "2-bit g0 codes in one word");
+        const uint32_t t = st[0];
+        const uint32_t p0 = ((t << 6) & 0xC0C0C0C0u) ^ 0x80808080u, p1 = ((t << 4) & 0xC0C0C0C0u) ^ 0x80808080u;
+        const uint32_t p2 = ((t << 2) & 0xC0C0C0C0u) ^ 0x80808080u, p3 = (t & 0xC0C0C0C0u) ^ 0x80808080u;
+        const uint32_t a = __byte_perm(p0, p1, 0x5140), c2 = __byte_perm(p2, p3, 0x5140);  // bytes 0, 1
+        w[(q * C0) >> 2] = __byte_perm(a, c2, 0x5410);
+        if constexpr (C0 > 4) w[(q * C0 + 4) >> 2] = __byte_perm(a, c2, 0x7632);
+        if constexpr (C0 > 8) {
+          const uint32_t b = __byte_perm(p0, p1, 0x7362), d = __byte_perm(p2, p3, 0x7362);  // bytes 2, 3
+          w[(q * C0 + 8) >> 2] = __byte_perm(b, d, 0x5410);
+          if constexpr (C0 > 12) w[(q * C0 + 12) >> 2] = __byte_perm(b, d, 0x7632);
+        }
       }
     }
   }
