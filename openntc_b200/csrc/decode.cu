@@ -630,9 +630,14 @@ __global__ void __launch_bounds__(kThreads, 1) decode_kernel(const __grid_consta
       ptx::ld16(lwin, acc);
       ptx::ld_wait();
       if (valid) {
+        // (float)sum * scale, saturated by the multiply; groups of four rows past the channel
+        // count (the same for every thread) are skipped
 #pragma unroll
-        for (int c = 0; c < kOutRows; c++)  // (float)sum * scale, saturated by the multiply
-          acc[c] = __saturatef(__fmul_rn(__fsub_rn(acc[c], 12582912.0f), so[c]));
+        for (int c0 = 0; c0 < kOutRows; c0 += 4)
+          if (c0 < C) {
+#pragma unroll
+            for (int c = c0; c < c0 + 4; c++) acc[c] = __saturatef(__fmul_rn(__fsub_rn(acc[c], 12582912.0f), so[c]));
+          }
         if (A.material) {
           store_material(A.out + i * 18, acc, C, A);
         } else {
